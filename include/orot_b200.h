@@ -1,0 +1,139 @@
+/*
+ * orot_b200.h -- C ABI of the B200 DEFLATE compression engine (liborot_b200.so).
+ *
+ * The first block of entry points has exactly the signatures, enum values and
+ * error conventions of orot's public DEFLATE compress API, so a program (or a
+ * cgo / ctypes / JNI binding) that calls orot for compression can link this
+ * library instead.  Each declaration cites the reference interface it
+ * replaces (include/orot/deflate.h in daramkun/orot).  All buffers are host
+ * memory owned by the caller; device memory is managed inside the library.
+ *
+ * The second block is this engine's own extension: batches of buffers kept
+ * on the device, compressed by one pass of kernels (optionally replayed from
+ * a CUDA graph), and a continuous-batching server.
+ */
+#ifndef OROT_B200_H
+#define OROT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* deflate_result -- include/orot/deflate.h:15-25 (same values) */
+typedef enum deflate_result {
+  DEFLATE_OK = 0,
+  DEFLATE_STREAM_END = 1,
+  DEFLATE_NEED_INPUT = 2,
+  DEFLATE_NEED_OUTPUT = 3,
+  DEFLATE_DATA_ERROR = -1,
+  DEFLATE_MEM_ERROR = -2,
+  DEFLATE_BUF_ERROR = -3,
+  DEFLATE_VERSION_ERROR = -4,
+  DEFLATE_PARAM_ERROR = -5
+} deflate_result;
+
+/* deflate_format -- include/orot/deflate.h:28-32 (same values) */
+typedef enum deflate_format {
+  DEFLATE_FORMAT_RAW = 0,  /* RFC 1951 */
+  DEFLATE_FORMAT_ZLIB = 1, /* RFC 1950, Adler-32 trailer */
+  DEFLATE_FORMAT_GZIP = 2  /* RFC 1952, CRC-32 trailer */
+} deflate_format;
+
+/* levels -- include/orot/deflate.h:35-39; values outside 0..12 are clamped
+ * exactly as src/deflate/lz77.cpp:33-34 does. */
+#define DEFLATE_LEVEL_STORE 0
+#define DEFLATE_LEVEL_FAST 1
+#define DEFLATE_LEVEL_DEFAULT 6
+#define DEFLATE_LEVEL_BETTER 9
+#define DEFLATE_LEVEL_MAX 12
+
+/* deflate_allocator -- include/orot/deflate.h:50-54 */
+typedef struct deflate_allocator {
+  void* (*alloc)(void* opaque, size_t size, size_t alignment);
+  void (*free)(void* opaque, void* ptr);
+  void* opaque;
+} deflate_allocator;
+
+/* Replaces deflate_set_allocator, include/orot/deflate.h:61.  Stored and
+ * otherwise unused, as in the reference (src/api/deflate_api.cpp:75-77):
+ * device memory never comes from a host allocator. */
+void deflate_set_allocator(const deflate_allocator* alloc);
+
+/* Replaces deflate_compress_bound, include/orot/deflate.h:66.
+ * n + n/4096 + n/16384 + n/2^25 + 13, plus 6 (zlib) or 18 (gzip). */
+size_t deflate_compress_bound(size_t in_size, deflate_format format);
+
+/* Replaces deflate_compress, include/orot/deflate.h:72-77.  One DEFLATE
+ * block for the whole input; levels 1-3 give byte-identical output to the
+ * reference.  Returns the compressed size, or 0 if out_capacity is below
+ * deflate_compress_bound() or on any device error. */
+size_t deflate_compress(const void* in, size_t in_size, void* out, size_t out_capacity, int level,
+                        deflate_format format);
+
+/* Replaces the parallel API, include/orot/deflate.h:122-145.  num_threads is
+ * accepted and ignored (the chunks run on the GPU); block_size 0 selects
+ * 128 KiB / 512 KiB / 1 MiB by level as src/parallel/parallel_compressor.cpp:16-20.
+ * deflate_parallel_compress returns 0 for a NULL context, or when the stream
+ * does not fit out_capacity. */
+typedef struct deflate_parallel_ctx deflate_parallel_ctx;
+deflate_parallel_ctx* deflate_parallel_new(int level, deflate_format format, int num_threads, size_t block_size);
+void deflate_parallel_free(deflate_parallel_ctx* ctx);
+size_t deflate_parallel_compress(deflate_parallel_ctx* ctx, const void* in, size_t in_size, void* out,
+                                 size_t out_capacity);
+
+/* Replace deflate_adler32 / deflate_crc32, include/orot/deflate.h:149-150.
+ * CRC-32 is the IEEE polynomial (the reference's scalar and ARM paths,
+ * src/simd/simd_detect.cpp:33-50). */
+uint32_t deflate_adler32(uint32_t initial, const void* data, size_t len);
+uint32_t deflate_crc32(uint32_t initial, const void* data, size_t len);
+
+/* ------------------------------------------------------------------------
+ * Extension: device-resident batches (no counterpart in the reference, whose
+ * only multi-buffer path is one deflate_compress call per buffer).
+ * ---------------------------------------------------------------------- */
+
+typedef struct deflate_gpu_batch deflate_gpu_batch;
+
+/* A batch owns device arenas and a CUDA stream on the current device. */
+deflate_gpu_batch* deflate_gpu_batch_new(void);
+void deflate_gpu_batch_free(deflate_gpu_batch* b);
+
+/* Copies `count` buffers (concatenated in host memory, sizes[i] bytes each)
+ * into device memory and plans them: each buffer becomes one independent
+ * stream with deflate_compress semantics (parallel = 0) or pigz chunking
+ * (parallel = 1, block_size as deflate_parallel_new).  Returns 0 on success. */
+int deflate_gpu_batch_load(deflate_gpu_batch* b, const void* host_concat, const size_t* sizes, size_t count, int level,
+                           deflate_format format, int parallel, size_t block_size);
+
+/* Runs the kernels on `cuda_stream` (a cudaStream_t, NULL = the batch's own
+ * stream) without host synchronisation.  use_graph != 0 replays a CUDA graph
+ * captured on first use.  Returns 0 on success. */
+int deflate_gpu_batch_run(deflate_gpu_batch* b, void* cuda_stream, int use_graph);
+
+/* Waits for the batch and copies the compressed sizes (0 = failed stream). */
+int deflate_gpu_batch_sizes(deflate_gpu_batch* b, size_t* out_sizes);
+
+/* Copies compressed stream i to host memory; returns its size or 0. */
+size_t deflate_gpu_batch_output(deflate_gpu_batch* b, size_t i, void* dst, size_t capacity);
+
+/* Number of kernel launches issued by the last deflate_gpu_batch_run. */
+int deflate_gpu_batch_launches(const deflate_gpu_batch* b);
+
+/* End-to-end batch from host buffers: copies in, compresses, copies every
+ * output back (deflate_compress semantics per buffer).  out_sizes[i] = 0
+ * marks a buffer whose output did not fit out_caps[i].  Returns the number of
+ * buffers compressed. */
+size_t deflate_gpu_compress_batch(const void* const* in, const size_t* in_sizes, void* const* out,
+                                  const size_t* out_caps, size_t* out_sizes, size_t count, int level,
+                                  deflate_format format);
+
+/* Last error message of the calling thread ("" if none). */
+const char* orot_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OROT_B200_H */

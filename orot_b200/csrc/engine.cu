@@ -1,0 +1,413 @@
+// engine.cu -- host side of the engine: planning, device arenas, launches,
+// and the C ABI declared in include/orot_b200.h.
+//
+// A compression pass takes a list of jobs (one per output stream), lays out
+// the Stream / Segment / Tile / Piece / CkBlock tables in one host buffer,
+// uploads it with a single copy and launches:
+//   fast-level LZ77 (kernels_fast.cu) and lazy-level LZ77 + Huffman
+//   (kernels_lazy.cu), block planning and zeroing, bit join, checksums and
+//   framing (kernels_common.cu).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "engine.cuh"
+#include "kernels.cuh"
+#include "engine_host.h"
+#include "../../include/orot_b200.h"
+
+namespace orotb {
+
+thread_local std::string g_err;
+void set_error(const std::string& e) { g_err = e; }
+
+#define CK(x)                                                                      \
+  do {                                                                             \
+    cudaError_t e_ = (x);                                                          \
+    if (e_ != cudaSuccess) {                                                       \
+      set_error(std::string(#x) + ": " + cudaGetErrorString(e_));                  \
+      return false;                                                                \
+    }                                                                              \
+  } while (0)
+
+size_t raw_bound(size_t n) { return n + (n >> 12) + (n >> 14) + (n >> 25) + 13; }
+size_t framed_bound(size_t n, int fmt) { return raw_bound(n) + (fmt == kFmtZlib ? 6 : fmt == kFmtGzip ? 18 : 0); }
+size_t default_block(int level) { return level <= 3 ? 131072 : level <= 6 ? 524288 : 1048576; }
+int clamp_level(int l) { return l < 0 ? 0 : l > 12 ? 12 : l; }
+
+bool DevBuf::ensure(size_t n) {
+  if (n <= cap) return true;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  size_t want = std::max(n, cap + cap / 2);
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    if (cudaMalloc(&p, n) != cudaSuccess) { cudaGetLastError(); p = nullptr; set_error("cudaMalloc failed"); return false; }
+    want = n;
+  }
+  cap = want;
+  return true;
+}
+void DevBuf::release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+
+bool HostBuf::ensure(size_t n) {
+  if (n <= cap) return true;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+  if (cudaMallocHost(&p, n) != cudaSuccess) { cudaGetLastError(); p = nullptr; set_error("cudaMallocHost failed"); return false; }
+  cap = n;
+  return true;
+}
+void HostBuf::release() { if (p) cudaFreeHost(p); p = nullptr; cap = 0; }
+
+Engine::Engine() {
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+  upload_crc_tables();
+  // Tile size override (bytes, multiple of 32, at most 64 KiB) for tests.
+  if (const char* v = std::getenv("OROT_B200_TILE")) {
+    const long t = std::strtol(v, nullptr, 10);
+    if (t >= 32 && t <= 65536 && t % 32 == 0) tile_override = uint32_t(t);
+  }
+}
+Engine::~Engine() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  for (DevBuf* b : {&d_in, &d_out, &d_scratch, &d_tables, &d_pack}) b->release();
+  h_tables.release();
+  h_stage.release();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// Tile size: 64 KiB, halved (down to 16 KiB) while the pass would leave the
+// GPU with fewer than ~8 tiles per SM.
+uint32_t Engine::pick_tile(uint64_t total_bytes) const {
+  uint32_t t = 65536;
+  const uint64_t want = uint64_t(sms) * 8;
+  while (t > 16384 && (total_bytes + t - 1) / t < want) t >>= 1;
+  if (tile_override) t = tile_override;
+  return t;
+}
+
+template <class T>
+static uint64_t put_table(std::vector<uint8_t>& buf, const std::vector<T>& v) {
+  const uint64_t off = align_up(buf.size(), 256);
+  buf.resize(off + v.size() * sizeof(T));
+  if (!v.empty()) std::memcpy(buf.data() + off, v.data(), v.size() * sizeof(T));
+  return off;
+}
+
+bool Engine::plan(const std::vector<Job>& jobs) {
+  streams.clear(); segs.clear(); tiles.clear(); cks.clear();
+  for (auto& l : lists) l.clear();
+  uint64_t total = 0;
+  for (const Job& j : jobs) total += j.in_len;
+  const uint32_t T = pick_tile(total);
+  uint64_t scratch = 0;
+  uint32_t npieces = 0;
+  for (size_t ji = 0; ji < jobs.size(); ++ji) {
+    const Job& j = jobs[ji];
+    Stream s{};
+    s.in_off = j.in_off;
+    s.in_len = j.in_len;
+    s.out_off = j.out_off;
+    s.out_cap = j.out_cap;
+    s.level = j.level;
+    s.fmt = uint32_t(j.fmt);
+    s.parallel = j.parallel ? 1 : 0;
+    s.seg_first = uint32_t(segs.size());
+    s.piece_first = npieces;
+    const int lv = clamp_level(j.level);
+    const uint64_t blk = j.parallel ? (j.block_size ? j.block_size : default_block(j.level)) : std::max<uint64_t>(j.in_len, 1);
+    const uint64_t nseg = j.in_len ? (j.in_len + blk - 1) / blk : 1;
+    for (uint64_t k = 0; k < nseg; ++k) {
+      Segment g{};
+      const uint64_t off = k * blk;
+      const uint64_t len = j.in_len ? std::min(blk, j.in_len - off) : 0;
+      if (len > 0xFFFFFFFFull - 65536) { set_error("segment larger than 4 GiB"); return false; }
+      g.in_off = j.in_off + off;
+      g.len = uint32_t(len);
+      g.stream = uint32_t(ji);
+      g.level = lv;
+      g.flags = (k + 1 == nseg ? kSegLast : 0) | (j.parallel ? 0 : kSegWholeBuf);
+      g.tile_first = uint32_t(tiles.size());
+      const int hb = lv <= 0 ? 0 : lv == 1 ? 12 : lv <= 3 ? 14 : 0;
+      const uint32_t H = hb ? (1u << hb) : 0;
+      if (lv > 0) {
+        const uint32_t nt = len ? uint32_t((len + T - 1) / T) : 1;
+        g.tile_count = nt;
+        const uint32_t seg_index = uint32_t(segs.size());
+        if (lv <= 3 && nt > 1) lists[hb == 12 ? kMulti12 : kMulti14].push_back(seg_index);
+        if (lv >= 4) lists[kLazySegs].push_back(seg_index);
+        for (uint32_t t = 0; t < nt; ++t) {
+          Tile tl{};
+          tl.seg = seg_index;
+          tl.start = t * T;
+          tl.len = uint32_t(std::min<uint64_t>(T, len - std::min<uint64_t>(len, uint64_t(t) * T)));
+          tl.index = t;
+          const uint64_t sb = tile_stream_bytes(tl.len);
+          tl.scratch = scratch;
+          scratch += 2 * sb;  // speculative + fix-up bit buffers
+          if (t > 0) {
+            tl.rec = scratch;
+            scratch += align_up(uint64_t((tl.len + 31) / 32) * sizeof(WinRec), 256);
+            tl.carry = tiles.back().slot;
+          }
+          if (t + 1 < nt && H) {
+            tl.slot = scratch;
+            scratch += uint64_t(H) * 4;
+          }
+          const uint32_t ti = uint32_t(tiles.size());
+          if (lv <= 3) {
+            lists[hb == 12 ? kWalk12 : kWalk14].push_back(ti);
+            if (t + 1 < nt) lists[hb == 12 ? kLast12 : kLast14].push_back(ti);
+          } else {
+            lists[kLazyTiles].push_back(ti);
+          }
+          tiles.push_back(tl);
+        }
+        if (lv >= 4) {
+          g.hdr_off = scratch;
+          scratch += 512;  // code-length header: at most ~ (5+5+4+19*3+320*7+...) bits
+        }
+      }
+      const uint32_t stored_pieces = std::max<uint32_t>(1, uint32_t((len + 65534) / 65535));
+      npieces += 1 + 2 * g.tile_count + 2 + 3 * stored_pieces;
+      segs.push_back(g);
+    }
+    s.seg_count = uint32_t(segs.size()) - s.seg_first;
+    s.piece_count = npieces - s.piece_first;
+    s.ck_first = uint32_t(cks.size());
+    if (j.fmt != kFmtRaw) {
+      for (uint64_t o = 0; o < j.in_len; o += 65536) {
+        CkBlock c{};
+        c.in_off = j.in_off + o;
+        c.len = uint32_t(std::min<uint64_t>(65536, j.in_len - o));
+        c.stream = uint32_t(ji);
+        cks.push_back(c);
+      }
+    }
+    s.ck_count = uint32_t(cks.size()) - s.ck_first;
+    streams.push_back(s);
+  }
+  n_pieces = npieces;
+  scratch_bytes = align_up(scratch + 256, 256);
+
+  // one host buffer, one upload
+  std::vector<uint8_t> buf;
+  off_streams = put_table(buf, streams);
+  off_segs = put_table(buf, segs);
+  off_tiles = put_table(buf, tiles);
+  off_ck = put_table(buf, cks);
+  for (int i = 0; i < kNumLists; ++i) off_lists[i] = put_table(buf, lists[i]);
+  off_counters = align_up(buf.size(), 256);
+  buf.resize(off_counters + 256, 0);
+  off_pieces = align_up(buf.size(), 256);
+  const uint64_t table_bytes = off_pieces + uint64_t(npieces) * sizeof(Piece) + 256;
+  if (!d_tables.ensure(table_bytes) || !h_tables.ensure(buf.size())) return false;
+  std::memcpy(h_tables.p, buf.data(), buf.size());
+  upload_bytes = buf.size();
+  if (!d_scratch.ensure(scratch_bytes)) return false;
+  return true;
+}
+
+Work Engine::work() const {
+  Work w{};
+  uint8_t* t = static_cast<uint8_t*>(d_tables.p);
+  w.in = static_cast<const uint8_t*>(d_in.p);
+  w.out = static_cast<uint8_t*>(d_out.p);
+  w.scratch = static_cast<uint8_t*>(d_scratch.p);
+  w.streams = reinterpret_cast<Stream*>(t + off_streams);
+  w.segs = reinterpret_cast<Segment*>(t + off_segs);
+  w.tiles = reinterpret_cast<Tile*>(t + off_tiles);
+  w.pieces = reinterpret_cast<Piece*>(t + off_pieces);
+  w.ck = reinterpret_cast<CkBlock*>(t + off_ck);
+  w.nstreams = uint32_t(streams.size());
+  w.nsegs = uint32_t(segs.size());
+  w.ntiles = uint32_t(tiles.size());
+  w.npieces = n_pieces;
+  w.nck = uint32_t(cks.size());
+  return w;
+}
+
+// Uploads the planned tables and launches every kernel of the pass on st.
+bool Engine::launch(cudaStream_t st) {
+  launches = 0;
+  uint8_t* t = static_cast<uint8_t*>(d_tables.p);
+  CK(cudaMemcpyAsync(t, h_tables.p, upload_bytes, cudaMemcpyHostToDevice, st));
+  const Work w = work();
+  uint32_t* counters = reinterpret_cast<uint32_t*>(t + off_counters);
+  auto list = [&](int i) { return reinterpret_cast<const uint32_t*>(t + off_lists[i]); };
+  const int hbs[2] = {12, 14};
+  for (int g = 0; g < 2; ++g) {
+    FastLists L{};
+    L.lastocc = list(g ? kLast14 : kLast12);
+    L.n_lastocc = uint32_t(lists[g ? kLast14 : kLast12].size());
+    L.multi = list(g ? kMulti14 : kMulti12);
+    L.n_multi = uint32_t(lists[g ? kMulti14 : kMulti12].size());
+    L.walk = list(g ? kWalk14 : kWalk12);
+    L.n_walk = uint32_t(lists[g ? kWalk14 : kWalk12].size());
+    L.counter = counters + g;
+    if (L.n_walk) {
+      launch_fast(w, L, hbs[g], st, sms);
+      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 2 : 0) + 1;
+    }
+  }
+  if (!lists[kLazyTiles].empty()) {
+    LazyLists L{};
+    L.tiles = list(kLazyTiles);
+    L.n_tiles = uint32_t(lists[kLazyTiles].size());
+    L.segs = list(kLazySegs);
+    L.n_segs = uint32_t(lists[kLazySegs].size());
+    L.counter = counters + 2;
+    launches += launch_lazy(w, L, st, sms);
+  }
+  launch_plan(w, st);
+  launches += 2;
+  launch_join(w, counters + 3, st, sms);
+  launches += w.npieces ? 1 : 0;
+  if (w.nck) {
+    launch_checksums(w, st);
+    launches += 2;
+  }
+  launch_frame(w, st);
+  launches += 1;
+  CK(cudaGetLastError());
+  return true;
+}
+
+bool Engine::ensure_io(uint64_t in_bytes, uint64_t out_bytes) {
+  return d_in.ensure(in_bytes + 64) && d_out.ensure(out_bytes + 64);
+}
+
+// Whole-buffer or pigz-style compression of one host buffer.
+size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel,
+                             size_t block) {
+  const size_t bound = framed_bound(n, fmt);
+  if (!ensure_io(align_up(n, 16), align_up(bound, 16))) return 0;
+  if (n) {
+    if (!h_stage.ensure(n)) return 0;
+    std::memcpy(h_stage.p, in, n);
+    if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) { set_error("H2D failed"); return 0; }
+  }
+  std::vector<Job> jobs(1);
+  jobs[0] = Job{0, n, 0, parallel ? std::min<uint64_t>(cap, bound) : bound, level, fmt, parallel, block};
+  if (!plan(jobs) || !launch(stream)) return 0;
+  Stream s{};
+  if (cudaMemcpyAsync(&s, static_cast<uint8_t*>(d_tables.p) + off_streams, sizeof s, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    set_error(std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
+    return 0;
+  }
+  if (s.error || s.out_size == 0 || s.out_size > cap) return 0;
+  if (!h_stage.ensure(s.out_size)) return 0;
+  if (cudaMemcpyAsync(h_stage.p, static_cast<uint8_t*>(d_out.p) + s.out_off, s.out_size, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    set_error("D2H failed");
+    return 0;
+  }
+  std::memcpy(out, h_stage.p, s.out_size);
+  return s.out_size;
+}
+
+uint32_t Engine::checksum_host(uint32_t init, const void* data, size_t n, bool adler) {
+  if (n == 0) return init;
+  if (!ensure_io(align_up(n, 16), 64) || !h_stage.ensure(n)) return init;
+  std::memcpy(h_stage.p, data, n);
+  // checksum blocks of the whole buffer
+  cks.clear();
+  for (uint64_t o = 0; o < n; o += 65536) {
+    CkBlock c{};
+    c.in_off = o;
+    c.len = uint32_t(std::min<uint64_t>(65536, n - o));
+    cks.push_back(c);
+  }
+  const size_t ck_bytes = cks.size() * sizeof(CkBlock);
+  if (!d_tables.ensure(ck_bytes + 256)) return init;
+  uint32_t* d_res = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(d_tables.p) + align_up(ck_bytes, 256));
+  Work w{};
+  w.in = static_cast<const uint8_t*>(d_in.p);
+  w.ck = static_cast<CkBlock*>(d_tables.p);
+  w.nck = uint32_t(cks.size());
+  uint32_t res = init;
+  if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+      cudaMemcpyAsync(d_tables.p, cks.data(), ck_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+    set_error("H2D failed");
+    return init;
+  }
+  launch_ck_single(w.ck, w.nck, n, init, adler ? 1 : 0, d_res, w, stream);
+  if (cudaMemcpyAsync(&res, d_res, 4, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    set_error("checksum failed");
+    return init;
+  }
+  return res;
+}
+
+std::mutex& global_mutex() { static std::mutex m; return m; }
+Engine& global_engine() { static Engine* e = new Engine(); return *e; }
+
+}  // namespace orotb
+
+// ====================================================================== C ABI
+using namespace orotb;
+
+struct deflate_parallel_ctx {
+  int level;
+  int fmt;
+  size_t block;
+};
+
+extern "C" {
+
+// Kept for ABI compatibility; like the reference, nothing allocates through it.
+static deflate_allocator g_user_alloc{};
+void deflate_set_allocator(const deflate_allocator* a) {
+  if (a) g_user_alloc = *a;
+  (void)g_user_alloc;
+}
+
+size_t deflate_compress_bound(size_t n, deflate_format f) { return framed_bound(n, int(f)); }
+
+size_t deflate_compress(const void* in, size_t n, void* out, size_t cap, int level, deflate_format f) {
+  const int fmt = int(f);
+  if (fmt < 0 || fmt > 2) return 0;
+  if (cap < framed_bound(n, fmt)) return 0;
+  if ((n && !in) || !out) return 0;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  return global_engine().compress_host(in, n, out, cap, level, fmt, false, 0);
+}
+
+deflate_parallel_ctx* deflate_parallel_new(int level, deflate_format f, int, size_t block) {
+  if (int(f) < 0 || int(f) > 2) return nullptr;
+  return new (std::nothrow) deflate_parallel_ctx{level, int(f), block};
+}
+void deflate_parallel_free(deflate_parallel_ctx* c) { delete c; }
+
+size_t deflate_parallel_compress(deflate_parallel_ctx* c, const void* in, size_t n, void* out, size_t cap) {
+  if (!c || (n && !in) || !out) return 0;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  return global_engine().compress_host(in, n, out, cap, c->level, c->fmt, true, c->block);
+}
+
+uint32_t deflate_crc32(uint32_t init, const void* data, size_t len) {
+  if (!data || !len) return init;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  return global_engine().checksum_host(init, data, len, false);
+}
+uint32_t deflate_adler32(uint32_t init, const void* data, size_t len) {
+  if (!data || !len) return init;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  return global_engine().checksum_host(init, data, len, true);
+}
+
+const char* orot_b200_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

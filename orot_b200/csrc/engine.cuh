@@ -1,0 +1,121 @@
+// engine.cuh -- data layout shared by the host planner and the sm_100a kernels.
+//
+// Work is described by three tables that live in HBM:
+//   Stream  : one compressed output (raw / zlib / gzip framing + trailer).
+//   Segment : a contiguous input range with its own LZ77 dictionary; it
+//             becomes exactly one DEFLATE block (the whole buffer for
+//             deflate_compress, one chunk for deflate_parallel_compress,
+//             src/compress/block_compressor.cpp:16-73 and
+//             src/parallel/parallel_compressor.cpp:65-84).
+//   Tile    : at most tile_size bytes of one segment, the unit one warp walks.
+//             Tiles of the same segment run concurrently: each starts with the
+//             hash-table state carried in from earlier tiles and parses from
+//             its own start; a sequential pass then moves the parse entry to
+//             where the previous tile's parse really ended.
+#pragma once
+#include <cstdint>
+
+namespace orotb {
+
+constexpr int kFmtRaw = 0, kFmtZlib = 1, kFmtGzip = 2;
+constexpr int kBlkStored = 0, kBlkFixed = 1, kBlkDynamic = 2;
+
+// Segment flags.
+constexpr uint32_t kSegLast = 1u;        // BFINAL block of its stream
+constexpr uint32_t kSegWholeBuf = 2u;    // whole-buffer rule: all-literal parse -> stored
+
+// Stream error codes written to Stream::error.
+constexpr uint32_t kErrNone = 0, kErrCapacity = 1, kErrInternal = 2;
+
+struct Stream {
+  uint64_t in_off;     // byte offset of the input in the input arena
+  uint64_t in_len;
+  uint64_t out_off;    // byte offset of the output slot (16-byte aligned)
+  uint64_t out_cap;    // caller capacity for the whole framed stream
+  uint32_t seg_first, seg_count;
+  uint32_t piece_first, piece_count;
+  int32_t level;       // unclamped caller level (gzip XFL uses it)
+  uint32_t fmt;
+  uint32_t parallel;   // 1: pigz framing (gzip XFL = 0)
+  uint32_t ck_first, ck_count;  // checksum blocks of this stream
+  // results
+  uint64_t out_size;   // framed bytes, 0 on error
+  uint32_t checksum;
+  uint32_t error;
+};
+
+struct Segment {
+  uint64_t in_off;     // absolute byte offset in the input arena
+  uint32_t len;
+  uint32_t stream;
+  uint32_t tile_first, tile_count;
+  uint32_t flags;
+  int32_t level;       // clamped 0..12
+  // dynamic blocks (levels 4+): header bits and end-of-block code
+  uint64_t hdr_off;    // scratch byte offset of the HLIT..code-lengths bits
+  uint32_t hdr_bits;
+  uint32_t eob;        // EOB code | (code length << 16)
+  // filled by the planner kernel
+  uint32_t block_type;
+  uint32_t pad0;
+  uint64_t bit_off;    // block start, in bits from the stream's raw start
+  uint64_t bits;       // block length in bits (stored: for its actual offset)
+};
+
+// Per-window parse record of a speculative tile walk (32 input positions).
+struct WinRec {
+  uint32_t entry;      // first parse position >= window start (tile-relative)
+  uint32_t bit;        // bit offset of that token in the tile's stream
+  uint32_t matches;    // match tokens before it
+  uint32_t pad;
+};
+
+struct Tile {
+  uint32_t seg;
+  uint32_t start;      // segment-relative
+  uint32_t len;
+  uint32_t index;      // index within the segment
+  uint64_t scratch;    // byte offset of this tile's bit buffers in the scratch arena
+  uint64_t rec;        // byte offset of WinRec[] (tiles with index > 0)
+  uint64_t carry;      // byte offset of the carried-in hash table (index > 0)
+  uint64_t slot;       // byte offset of this tile's published table (index < count-1)
+  // speculative walk (entry = tile start)
+  uint32_t spec_bits, spec_matches, spec_exit, spec_tokens;
+  // resolved parse: piece A = fix-up bits [0, fix_bits) from the fix-up
+  // buffer, piece B = speculative bits [splice_bit, spec_bits)
+  uint32_t fix_bits, splice_bit, fin_matches, fin_exit;
+};
+
+// A bit-range copy for the join kernel.  src == nullptr means "write the
+// low nbits of value".
+struct Piece {
+  const uint32_t* src;  // 4-byte aligned source words
+  uint32_t* dst;        // the stream's output slot (16-byte aligned)
+  uint64_t src_bit;     // first bit within src
+  uint64_t dst_bit;     // first bit within dst
+  uint32_t nbits;
+  uint32_t value;
+};
+
+// Checksum block: a range of one stream's input.
+struct CkBlock {
+  uint64_t in_off;     // absolute
+  uint32_t len;
+  uint32_t stream;
+  uint32_t crc;        // raw CRC register from 0 (no conditioning)
+  uint32_t a, b;       // Adler partial sums mod 65521
+  uint32_t pad;
+};
+
+// Limits.
+constexpr int kMaxTileLog2 = 16;           // 64 KiB tiles at most
+constexpr int kWindow = 32;
+
+__host__ __device__ inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+// Worst case bits of a tile's fixed-Huffman token stream: a literal costs at
+// most 9 bits and a match at most 25 bits per 3 covered bytes, so 9 bits per
+// input byte plus one match (31 bits) hanging over the tile end.
+__host__ __device__ inline uint64_t tile_stream_bytes(uint32_t tile_len) { return align_up(uint64_t(tile_len) * 9 / 8 + 64, 128); }
+
+}  // namespace orotb

@@ -1,0 +1,90 @@
+// engine_host.h -- host-side engine object shared by the C ABI, the batch API
+// and the server.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "engine.cuh"
+#include "kernels.cuh"
+
+namespace orotb {
+
+void set_error(const std::string& e);
+size_t raw_bound(size_t n);
+size_t framed_bound(size_t n, int fmt);
+size_t default_block(int level);
+int clamp_level(int l);
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  bool ensure(size_t n);
+  void release();
+};
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  bool ensure(size_t n);
+  void release();
+};
+
+// One output stream to produce.
+struct Job {
+  uint64_t in_off;      // in the input arena (16-byte aligned)
+  uint64_t in_len;
+  uint64_t out_off;     // in the output arena (16-byte aligned)
+  uint64_t out_cap;
+  int level;
+  int fmt;
+  bool parallel;        // pigz chunking instead of one block per buffer
+  uint64_t block_size;  // chunk size for parallel (0 = by level)
+};
+
+enum ListId {
+  kLast12, kMulti12, kWalk12,
+  kLast14, kMulti14, kWalk14,
+  kLazyTiles, kLazySegs,
+  kNumLists
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  bool ensure_io(uint64_t in_bytes, uint64_t out_bytes);
+  bool plan(const std::vector<Job>& jobs);
+  bool launch(cudaStream_t st);
+  Work work() const;
+  size_t compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel, size_t block);
+  uint32_t checksum_host(uint32_t init, const void* data, size_t n, bool adler);
+  uint32_t pick_tile(uint64_t total_bytes) const;
+
+  int device = 0, sms = 148;
+  cudaStream_t stream = nullptr;
+  DevBuf d_in, d_out, d_scratch, d_tables, d_pack;
+  HostBuf h_tables, h_stage;
+  cudaGraphExec_t graph_exec = nullptr;
+  uint32_t tile_override = 0;
+
+  // planned tables (host copies)
+  std::vector<Stream> streams;
+  std::vector<Segment> segs;
+  std::vector<Tile> tiles;
+  std::vector<CkBlock> cks;
+  std::vector<uint32_t> lists[kNumLists];
+  uint32_t n_pieces = 0;
+  uint64_t scratch_bytes = 0, upload_bytes = 0;
+  uint64_t off_streams = 0, off_segs = 0, off_tiles = 0, off_ck = 0, off_pieces = 0, off_counters = 0;
+  uint64_t off_lists[kNumLists] = {};
+  int launches = 0;
+};
+
+std::mutex& global_mutex();
+Engine& global_engine();
+
+}  // namespace orotb

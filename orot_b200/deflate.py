@@ -1,0 +1,223 @@
+"""Python mirror of orot's DEFLATE compress API over liborot_b200.so.
+
+Names, defaults and error behaviour follow the reference's C++ wrapper
+(include/orot/deflate.h:184-389 in daramkun/orot): `compress` raises `Error`
+with DEFLATE_BUF_ERROR when the C call returns 0, `ParallelCompressor`
+defaults to gzip, `adler32` / `crc32` take the initial value last.  Every call
+goes through the C ABI of include/orot_b200.h into the CUDA kernels; there is
+no host fallback, and importing this module without the built library or
+without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from typing import Sequence
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liborot_b200.so")
+_lib = None
+
+DEFLATE_OK = 0
+DEFLATE_MEM_ERROR = -2
+DEFLATE_BUF_ERROR = -3
+DEFLATE_PARAM_ERROR = -5
+
+
+class Format(enum.IntEnum):
+    Raw = 0
+    Zlib = 1
+    Gzip = 2
+
+
+class Level:
+    Store = 0
+    Fast = 1
+    Default = 6
+    Better = 9
+    Max = 12
+
+
+class Error(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Loads liborot_b200.so once; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is not built; run `python -m orot_b200.build`")
+    L = ctypes.CDLL(_LIB_PATH)
+    c = ctypes
+    L.deflate_compress_bound.restype = c.c_size_t
+    L.deflate_compress_bound.argtypes = [c.c_size_t, c.c_int]
+    L.deflate_compress.restype = c.c_size_t
+    L.deflate_compress.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.c_int, c.c_int]
+    L.deflate_parallel_new.restype = c.c_void_p
+    L.deflate_parallel_new.argtypes = [c.c_int, c.c_int, c.c_int, c.c_size_t]
+    L.deflate_parallel_free.argtypes = [c.c_void_p]
+    L.deflate_parallel_compress.restype = c.c_size_t
+    L.deflate_parallel_compress.argtypes = [c.c_void_p, c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t]
+    L.deflate_crc32.restype = c.c_uint32
+    L.deflate_crc32.argtypes = [c.c_uint32, c.c_void_p, c.c_size_t]
+    L.deflate_adler32.restype = c.c_uint32
+    L.deflate_adler32.argtypes = [c.c_uint32, c.c_void_p, c.c_size_t]
+    L.orot_b200_last_error.restype = c.c_char_p
+    L.deflate_gpu_batch_new.restype = c.c_void_p
+    L.deflate_gpu_batch_free.argtypes = [c.c_void_p]
+    L.deflate_gpu_batch_load.restype = c.c_int
+    L.deflate_gpu_batch_load.argtypes = [c.c_void_p, c.c_void_p, c.POINTER(c.c_size_t), c.c_size_t, c.c_int,
+                                         c.c_int, c.c_int, c.c_size_t]
+    L.deflate_gpu_batch_run.restype = c.c_int
+    L.deflate_gpu_batch_run.argtypes = [c.c_void_p, c.c_void_p, c.c_int]
+    L.deflate_gpu_batch_sizes.restype = c.c_int
+    L.deflate_gpu_batch_sizes.argtypes = [c.c_void_p, c.POINTER(c.c_size_t)]
+    L.deflate_gpu_batch_output.restype = c.c_size_t
+    L.deflate_gpu_batch_output.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t]
+    L.deflate_gpu_batch_launches.restype = c.c_int
+    L.deflate_gpu_batch_launches.argtypes = [c.c_void_p]
+    L.deflate_gpu_compress_batch.restype = c.c_size_t
+    L.deflate_gpu_compress_batch.argtypes = [c.POINTER(c.c_void_p), c.POINTER(c.c_size_t), c.POINTER(c.c_void_p),
+                                             c.POINTER(c.c_size_t), c.POINTER(c.c_size_t), c.c_size_t, c.c_int,
+                                             c.c_int]
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().orot_b200_last_error().decode()
+
+
+def _ptr(buf) -> tuple[int, int, object]:
+    """(address, length, keepalive) of a bytes-like or numpy buffer."""
+    try:
+        import numpy as np
+        if isinstance(buf, np.ndarray):
+            a = np.ascontiguousarray(buf).view(np.uint8).reshape(-1)
+            return a.ctypes.data, a.size, a
+    except ImportError:  # pragma: no cover
+        pass
+    mv = memoryview(buf).cast("B")
+    if mv.readonly:
+        b = ctypes.create_string_buffer(bytes(mv), len(mv))
+        return ctypes.addressof(b), len(mv), b
+    arr = (ctypes.c_char * len(mv)).from_buffer(mv)
+    return ctypes.addressof(arr), len(mv), (arr, mv)
+
+
+def compress_bound(n: int, format: Format = Format.Zlib) -> int:
+    return lib().deflate_compress_bound(n, int(format))
+
+
+def compress(data, level: int = Level.Default, format: Format = Format.Zlib) -> bytes:
+    """deflate_compress over the whole input (include/orot/deflate.h:219-235)."""
+    L = lib()
+    addr, n, keep = _ptr(data)
+    bound = L.deflate_compress_bound(n, int(format))
+    out = ctypes.create_string_buffer(bound)
+    r = L.deflate_compress(addr if n else None, n, out, bound, int(level), int(format))
+    del keep
+    if r == 0:
+        raise Error(DEFLATE_BUF_ERROR, "deflate::compress: output buffer overflow " + last_error())
+    return out.raw[:r]
+
+
+class ParallelCompressor:
+    """pigz-style compressor (include/orot/deflate.h:351-376)."""
+
+    def __init__(self, level: int = Level.Default, fmt: Format = Format.Gzip, threads: int = 0, block_size: int = 0):
+        self._ctx = lib().deflate_parallel_new(int(level), int(fmt), int(threads), int(block_size))
+        if not self._ctx:
+            raise Error(DEFLATE_MEM_ERROR, "ParallelCompressor: allocation failed")
+        self.level, self.fmt, self.block_size = level, fmt, block_size
+
+    def compress(self, data) -> bytes:
+        L = lib()
+        addr, n, keep = _ptr(data)
+        bound = L.deflate_compress_bound(n, int(Format.Gzip))
+        out = ctypes.create_string_buffer(bound)
+        r = L.deflate_parallel_compress(self._ctx, addr if n else None, n, out, bound)
+        del keep
+        if r == 0:
+            raise Error(DEFLATE_BUF_ERROR, "ParallelCompressor::compress: buffer overflow " + last_error())
+        return out.raw[:r]
+
+    def close(self) -> None:
+        if self._ctx:
+            lib().deflate_parallel_free(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+
+def adler32(data, init: int = 1) -> int:
+    addr, n, keep = _ptr(data)
+    r = lib().deflate_adler32(init, addr if n else None, n)
+    del keep
+    return r
+
+
+def crc32(data, init: int = 0) -> int:
+    addr, n, keep = _ptr(data)
+    r = lib().deflate_crc32(init, addr if n else None, n)
+    del keep
+    return r
+
+
+class DeviceBatch:
+    """Buffers kept on the device and compressed by one pass of kernels."""
+
+    def __init__(self):
+        self._b = lib().deflate_gpu_batch_new()
+        if not self._b:
+            raise Error(DEFLATE_MEM_ERROR, "batch: " + last_error())
+        self.count = 0
+
+    def load(self, concat, sizes: Sequence[int], level: int, format: Format, parallel: bool = False,
+             block_size: int = 0) -> None:
+        addr, n, keep = _ptr(concat)
+        arr = (ctypes.c_size_t * len(sizes))(*sizes)
+        r = lib().deflate_gpu_batch_load(self._b, addr, arr, len(sizes), int(level), int(format), int(parallel),
+                                         int(block_size))
+        del keep
+        if r != 0:
+            raise Error(DEFLATE_PARAM_ERROR, "batch load: " + last_error())
+        self.count = len(sizes)
+
+    def run(self, stream: int = 0, graph: bool = False) -> None:
+        r = lib().deflate_gpu_batch_run(self._b, ctypes.c_void_p(stream or None), int(graph))
+        if r != 0:
+            raise Error(DEFLATE_PARAM_ERROR, "batch run: " + last_error())
+
+    def sizes(self) -> list[int]:
+        arr = (ctypes.c_size_t * self.count)()
+        if lib().deflate_gpu_batch_sizes(self._b, arr) != 0:
+            raise Error(DEFLATE_PARAM_ERROR, "batch sizes: " + last_error())
+        return list(arr)
+
+    def output(self, i: int, size: int) -> bytes:
+        buf = ctypes.create_string_buffer(max(size, 1))
+        r = lib().deflate_gpu_batch_output(self._b, i, buf, size)
+        return buf.raw[:r]
+
+    def launches(self) -> int:
+        return lib().deflate_gpu_batch_launches(self._b)
+
+    def close(self) -> None:
+        if self._b:
+            lib().deflate_gpu_batch_free(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
