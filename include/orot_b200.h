@@ -122,6 +122,14 @@ size_t deflate_gpu_batch_output(deflate_gpu_batch* b, size_t i, void* dst, size_
 /* Number of kernel launches issued by the last deflate_gpu_batch_run. */
 int deflate_gpu_batch_launches(const deflate_gpu_batch* b);
 
+/* Per-phase timing: with profiling on, each run records CUDA events between
+ * kernel phases (graph replay is disabled while on).  phase_ms fills
+ * ms[0..n) with the milliseconds of each phase of the last run and returns
+ * n (needs max >= n); deflate_gpu_phase_name(i) names phase i. */
+int deflate_gpu_batch_profile(deflate_gpu_batch* b, int enable);
+int deflate_gpu_batch_phase_ms(deflate_gpu_batch* b, float* ms, int max);
+const char* deflate_gpu_phase_name(int i);
+
 /* End-to-end batch from host buffers: copies in, compresses, copies every
  * output back (deflate_compress semantics per buffer).  out_sizes[i] = 0
  * marks a buffer whose output did not fit out_caps[i].  Returns the number of
@@ -129,6 +137,19 @@ int deflate_gpu_batch_launches(const deflate_gpu_batch* b);
 size_t deflate_gpu_compress_batch(const void* const* in, const size_t* in_sizes, void* const* out,
                                   const size_t* out_caps, size_t* out_sizes, size_t count, int level,
                                   deflate_format format);
+
+/* End-to-end batch from one concatenated host buffer (sizes[i] bytes each,
+ * back to back): one host-to-device copy (DMA straight from in_concat when it
+ * is pinned), one pass of kernels, outputs packed on the device at 16-byte
+ * aligned offsets and copied back with one transfer into out_packed.
+ * out_offsets needs count + 1 entries (the last is the packed total);
+ * out_sizes[i] = 0 marks a failed stream.  Returns the packed byte count, or
+ * 0 on error (including out_capacity below the packed total; size it with
+ * deflate_gpu_packed_bound). */
+size_t deflate_gpu_compress_packed(const void* in_concat, const size_t* in_sizes, size_t count, int level,
+                                   deflate_format format, void* out_packed, size_t out_capacity, uint64_t* out_offsets,
+                                   size_t* out_sizes);
+size_t deflate_gpu_packed_bound(const size_t* in_sizes, size_t count, deflate_format format);
 
 /* Last error message of the calling thread ("" if none). */
 const char* orot_b200_last_error(void);

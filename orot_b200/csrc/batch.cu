@@ -75,9 +75,12 @@ static void drop_graph(deflate_gpu_batch* b) {
   b->graph = nullptr;
 }
 
-// Lays out `count` buffers, uploads them, plans the pass.
-static bool batch_setup(deflate_gpu_batch* b, const void* const* in, const size_t* sizes, size_t count, int level,
-                        int fmt, bool parallel, size_t block) {
+// Lays out `count` buffers, uploads them, plans the pass.  With `concat`
+// set, the buffers are back to back in caller memory and are copied to the
+// device in one transfer (DMA straight from the caller when it is pinned);
+// otherwise each buffer is staged at a 16-byte aligned offset.
+static bool batch_setup(deflate_gpu_batch* b, const void* const* in, const uint8_t* concat, const size_t* sizes,
+                        size_t count, int level, int fmt, bool parallel, size_t block, cudaStream_t st) {
   Engine& e = b->eng;
   drop_graph(b);
   b->jobs.assign(count, Job{});
@@ -87,24 +90,64 @@ static bool batch_setup(deflate_gpu_batch* b, const void* const* in, const size_
     j.in_off = in_total;
     j.in_len = sizes[i];
     j.out_off = out_total;
-    j.out_cap = framed_bound(sizes[i], fmt);
+    j.out_cap = parallel ? parallel_bound(sizes[i], fmt, level, block) : framed_bound(sizes[i], fmt);
     j.level = level;
     j.fmt = fmt;
     j.parallel = parallel;
     j.block_size = block;
-    in_total += align_up(sizes[i], 16);
+    in_total += concat ? sizes[i] : align_up(sizes[i], 16);
     out_total += align_up(j.out_cap, 16);
   }
-  if (!e.ensure_io(in_total, out_total) || !e.h_stage.ensure(std::max<uint64_t>(in_total, 16))) return false;
-  uint8_t* st = static_cast<uint8_t*>(e.h_stage.p);
-  for (size_t i = 0; i < count; ++i)
-    if (sizes[i]) std::memcpy(st + b->jobs[i].in_off, in[i], sizes[i]);
-  if (in_total && cudaMemcpyAsync(e.d_in.p, st, in_total, cudaMemcpyHostToDevice, e.stream) != cudaSuccess) {
-    set_error("H2D failed");
+  if (!e.ensure_io(in_total, out_total)) return false;
+  if (concat) {
+    if (in_total && cudaMemcpyAsync(e.d_in.p, concat, in_total, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      set_error("H2D failed");
+      return false;
+    }
+  } else {
+    if (!e.h_stage.ensure(std::max<uint64_t>(in_total, 16))) return false;
+    uint8_t* sp = static_cast<uint8_t*>(e.h_stage.p);
+    for (size_t i = 0; i < count; ++i)
+      if (sizes[i]) std::memcpy(sp + b->jobs[i].in_off, in[i], sizes[i]);
+    if (in_total && cudaMemcpyAsync(e.d_in.p, sp, in_total, cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      set_error("H2D failed");
+      return false;
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) { set_error("H2D sync failed"); return false; }
+  }
+  return e.plan(b->jobs);
+}
+
+// Packs every stream's output at 16-byte aligned offsets in e.d_pack and
+// copies sizes + offsets + packed bytes to the host.
+static bool batch_pack_to_host(deflate_gpu_batch* b, cudaStream_t st, void* host_out, size_t host_cap,
+                               uint64_t* offsets, size_t* sizes_out, uint64_t* total_out) {
+  Engine& e = b->eng;
+  const Work w = e.work();
+  const size_t count = e.streams.size();
+  uint64_t out_total = 0;
+  for (const Job& j : b->jobs) out_total += align_up(j.out_cap, 16);
+  if (!e.d_pack.ensure(align_up(out_total, 256) + (count + 1) * 8 + 256)) return false;
+  uint64_t* d_off = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(e.d_pack.p) + align_up(out_total, 256));
+  k_pack_offsets<<<1, 1024, 0, st>>>(w.streams, w.nstreams, d_off);
+  k_pack<<<w.nstreams, 256, 0, st>>>(w.streams, w.nstreams, d_off, w.out, static_cast<uint8_t*>(e.d_pack.p));
+  std::vector<Stream> s(count);
+  if (cudaMemcpyAsync(s.data(), w.streams, count * sizeof(Stream), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(offsets, d_off, (count + 1) * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
+    set_error("D2H failed");
     return false;
   }
-  if (cudaStreamSynchronize(e.stream) != cudaSuccess) { set_error("H2D sync failed"); return false; }
-  return e.plan(b->jobs);
+  const uint64_t total = offsets[count];
+  if (total > host_cap) { set_error("packed output larger than the host buffer"); return false; }
+  if (total && (cudaMemcpyAsync(host_out, e.d_pack.p, total, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)) {
+    set_error("D2H failed");
+    return false;
+  }
+  for (size_t i = 0; i < count; ++i) sizes_out[i] = s[i].error ? 0 : s[i].out_size;
+  *total_out = total;
+  return true;
 }
 
 extern "C" {
@@ -123,7 +166,9 @@ int deflate_gpu_batch_load(deflate_gpu_batch* b, const void* concat, const size_
   std::vector<const void*> ptrs(count);
   const uint8_t* p = static_cast<const uint8_t*>(concat);
   for (size_t i = 0; i < count; ++i) { ptrs[i] = p; p += sizes[i]; }
-  return batch_setup(b, ptrs.data(), sizes, count, level, int(format), parallel != 0, block_size) ? 0 : -1;
+  return batch_setup(b, ptrs.data(), nullptr, sizes, count, level, int(format), parallel != 0, block_size, b->eng.stream)
+             ? 0
+             : -1;
 }
 
 int deflate_gpu_batch_run(deflate_gpu_batch* b, void* cuda_stream, int use_graph) {
@@ -196,6 +241,26 @@ size_t deflate_gpu_batch_output(deflate_gpu_batch* b, size_t i, void* dst, size_
 
 int deflate_gpu_batch_launches(const deflate_gpu_batch* b) { return b ? b->launches : 0; }
 
+int deflate_gpu_batch_profile(deflate_gpu_batch* b, int enable) {
+  if (!b) return -1;
+  b->eng.marks.on = enable != 0;
+  drop_graph(b);  // a captured graph carries no event records
+  return 0;
+}
+
+int deflate_gpu_batch_phase_ms(deflate_gpu_batch* b, float* ms, int max) {
+  if (!b || !ms || max < int(kNumPhases)) return -1;
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+  b->eng.phase_ms(ms);
+  return int(kNumPhases);
+}
+
+const char* deflate_gpu_phase_name(int i) {
+  static const char* names[kNumPhases] = {"hash_carry", "walk", "fixup", "lazy_match", "lazy_huffman",
+                                          "lazy_encode", "plan", "join", "checksum", "frame"};
+  return i >= 0 && i < int(kNumPhases) ? names[i] : "";
+}
+
 size_t deflate_gpu_compress_batch(const void* const* in, const size_t* in_sizes, void* const* out, const size_t* out_caps,
                                   size_t* out_sizes, size_t count, int level, deflate_format format) {
   if (!count) return 0;
@@ -204,43 +269,52 @@ size_t deflate_gpu_compress_batch(const void* const* in, const size_t* in_sizes,
   static deflate_gpu_batch* gb = new deflate_gpu_batch();
   deflate_gpu_batch* b = gb;
   Engine& e = b->eng;
-  if (!batch_setup(b, in, in_sizes, count, level, int(format), false, 0)) return 0;
+  if (!batch_setup(b, in, nullptr, in_sizes, count, level, int(format), false, 0, e.stream)) return 0;
   if (!e.launch(e.stream)) return 0;
-  // pack on the device, one copy back
-  const Work w = e.work();
-  DevBuf& pk = e.d_pack;
-  uint64_t out_total = 0;
-  for (const Job& j : b->jobs) out_total += align_up(j.out_cap, 16);
-  if (!pk.ensure(out_total + 16 + (count + 1) * 8)) return 0;
-  uint64_t* d_off = reinterpret_cast<uint64_t*>(static_cast<uint8_t*>(pk.p) + align_up(out_total, 256));
-  k_pack_offsets<<<1, 1024, 0, e.stream>>>(w.streams, w.nstreams, d_off);
-  k_pack<<<w.nstreams, 256, 0, e.stream>>>(w.streams, w.nstreams, d_off, w.out, static_cast<uint8_t*>(pk.p));
-  std::vector<Stream> s(count);
   std::vector<uint64_t> off(count + 1);
-  if (cudaMemcpyAsync(s.data(), w.streams, count * sizeof(Stream), cudaMemcpyDeviceToHost, e.stream) != cudaSuccess ||
-      cudaMemcpyAsync(off.data(), d_off, (count + 1) * 8, cudaMemcpyDeviceToHost, e.stream) != cudaSuccess ||
-      cudaStreamSynchronize(e.stream) != cudaSuccess) {
-    set_error("D2H failed");
-    return 0;
-  }
-  if (!e.h_stage.ensure(off[count] + 16)) return 0;
-  if (off[count] && (cudaMemcpyAsync(e.h_stage.p, pk.p, off[count], cudaMemcpyDeviceToHost, e.stream) != cudaSuccess ||
-                     cudaStreamSynchronize(e.stream) != cudaSuccess)) {
-    set_error("D2H failed");
-    return 0;
-  }
+  std::vector<size_t> sz(count);
+  uint64_t bound = 0;
+  for (const Job& j : b->jobs) bound += align_up(j.out_cap, 16);
+  if (!e.h_stage.ensure(bound + 16)) return 0;
+  uint64_t total = 0;
+  if (!batch_pack_to_host(b, e.stream, e.h_stage.p, bound + 16, off.data(), sz.data(), &total)) return 0;
   size_t done = 0;
   for (size_t i = 0; i < count; ++i) {
-    const uint64_t n = s[i].error ? 0 : s[i].out_size;
-    if (n && n <= out_caps[i]) {
-      std::memcpy(out[i], static_cast<uint8_t*>(e.h_stage.p) + off[i], n);
-      out_sizes[i] = n;
+    if (sz[i] && sz[i] <= out_caps[i]) {
+      std::memcpy(out[i], static_cast<uint8_t*>(e.h_stage.p) + off[i], sz[i]);
+      out_sizes[i] = sz[i];
       ++done;
     } else {
       out_sizes[i] = 0;
     }
   }
   return done;
+}
+
+size_t deflate_gpu_compress_packed(const void* in_concat, const size_t* in_sizes, size_t count, int level,
+                                   deflate_format format, void* out_packed, size_t out_capacity, uint64_t* out_offsets,
+                                   size_t* out_sizes) {
+  if (!count || !in_sizes || !out_packed || !out_offsets || !out_sizes || int(format) < 0 || int(format) > 2) return 0;
+  uint64_t total_in = 0;
+  for (size_t i = 0; i < count; ++i) total_in += in_sizes[i];
+  if (total_in && !in_concat) return 0;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  static deflate_gpu_batch* gb = new deflate_gpu_batch();
+  deflate_gpu_batch* b = gb;
+  Engine& e = b->eng;
+  if (!batch_setup(b, nullptr, static_cast<const uint8_t*>(in_concat), in_sizes, count, level, int(format), false, 0,
+                   e.stream))
+    return 0;
+  if (!e.launch(e.stream)) return 0;
+  uint64_t total = 0;
+  if (!batch_pack_to_host(b, e.stream, out_packed, out_capacity, out_offsets, out_sizes, &total)) return 0;
+  return size_t(total);
+}
+
+size_t deflate_gpu_packed_bound(const size_t* in_sizes, size_t count, deflate_format format) {
+  uint64_t t = 0;
+  for (size_t i = 0; i < count; ++i) t += align_up(framed_bound(in_sizes[i], int(format)), 16);
+  return size_t(t);
 }
 
 }  // extern "C"

@@ -140,12 +140,11 @@ bool Engine::plan(const std::vector<Job>& jobs) {
       g.tile_first = uint32_t(tiles.size());
       const int hb = lv <= 0 ? 0 : lv == 1 ? 12 : lv <= 3 ? 14 : 0;
       const uint32_t H = hb ? (1u << hb) : 0;
-      if (lv > 0) {
+      if (lv > 0 && lv <= 3) {
         const uint32_t nt = len ? uint32_t((len + T - 1) / T) : 1;
         g.tile_count = nt;
         const uint32_t seg_index = uint32_t(segs.size());
-        if (lv <= 3 && nt > 1) lists[hb == 12 ? kMulti12 : kMulti14].push_back(seg_index);
-        if (lv >= 4) lists[kLazySegs].push_back(seg_index);
+        if (nt > 1) lists[hb == 12 ? kMulti12 : kMulti14].push_back(seg_index);
         for (uint32_t t = 0; t < nt; ++t) {
           Tile tl{};
           tl.seg = seg_index;
@@ -158,25 +157,45 @@ bool Engine::plan(const std::vector<Job>& jobs) {
           if (t > 0) {
             tl.rec = scratch;
             scratch += align_up(uint64_t((tl.len + 31) / 32) * sizeof(WinRec), 256);
+            tl.cand = scratch;
+            scratch += align_up(uint64_t(tl.len) * 2 + 64, 256);
             tl.carry = tiles.back().slot;
           }
-          if (t + 1 < nt && H) {
+          if (t + 1 < nt) {
             tl.slot = scratch;
             scratch += uint64_t(H) * 4;
           }
           const uint32_t ti = uint32_t(tiles.size());
-          if (lv <= 3) {
-            lists[hb == 12 ? kWalk12 : kWalk14].push_back(ti);
-            if (t + 1 < nt) lists[hb == 12 ? kLast12 : kLast14].push_back(ti);
-          } else {
-            lists[kLazyTiles].push_back(ti);
-          }
+          lists[hb == 12 ? kWalk12 : kWalk14].push_back(ti);
+          if (t + 1 < nt) lists[hb == 12 ? kLast12 : kLast14].push_back(ti);
           tiles.push_back(tl);
         }
-        if (lv >= 4) {
-          g.hdr_off = scratch;
-          scratch += 512;  // code-length header: at most ~ (5+5+4+19*3+320*7+...) bits
+      } else if (lv >= 4) {
+        // independent 8 KiB tiles, each with its own token words and histogram
+        const uint32_t LT = kLazyTile;
+        const uint32_t nt = len ? uint32_t((len + LT - 1) / LT) : 1;
+        g.tile_count = nt;
+        const uint32_t seg_index = uint32_t(segs.size());
+        lists[kLazySegs].push_back(seg_index);
+        for (uint32_t t = 0; t < nt; ++t) {
+          Tile tl{};
+          tl.seg = seg_index;
+          tl.start = t * LT;
+          tl.len = uint32_t(std::min<uint64_t>(LT, len - std::min<uint64_t>(len, uint64_t(t) * LT)));
+          tl.index = t;
+          tl.scratch = scratch;
+          scratch += lazy_stream_bytes(tl.len);
+          tl.tok = scratch;
+          scratch += align_up(uint64_t(tl.len) * 4 + 4, 256);
+          tl.hist = scratch;
+          scratch += 320 * 4;
+          lists[kLazyTiles].push_back(uint32_t(tiles.size()));
+          tiles.push_back(tl);
         }
+        g.codes = scratch;
+        scratch += 320 * 4;
+        g.hdr_off = scratch;
+        scratch += 1024;
       }
       const uint32_t stored_pieces = std::max<uint32_t>(1, uint32_t((len + 65534) / 65535));
       npieces += 1 + 2 * g.tile_count + 2 + 3 * stored_pieces;
@@ -241,7 +260,13 @@ Work Engine::work() const {
 bool Engine::launch(cudaStream_t st) {
   launches = 0;
   uint8_t* t = static_cast<uint8_t*>(d_tables.p);
+  marks.n = 0;
+  if (marks.on && !made_events) {
+    for (auto& e : marks.ev) cudaEventCreate(&e);
+    made_events = true;
+  }
   CK(cudaMemcpyAsync(t, h_tables.p, upload_bytes, cudaMemcpyHostToDevice, st));
+  marks.mark(-1, st);
   const Work w = work();
   uint32_t* counters = reinterpret_cast<uint32_t*>(t + off_counters);
   auto list = [&](int i) { return reinterpret_cast<const uint32_t*>(t + off_lists[i]); };
@@ -254,9 +279,9 @@ bool Engine::launch(cudaStream_t st) {
     L.n_multi = uint32_t(lists[g ? kMulti14 : kMulti12].size());
     L.walk = list(g ? kWalk14 : kWalk12);
     L.n_walk = uint32_t(lists[g ? kWalk14 : kWalk12].size());
-    L.counter = counters + g;
+    L.counter = counters + g;  // walk: 0/1; fix-up round 1: 4/5 (counter + 4)
     if (L.n_walk) {
-      launch_fast(w, L, hbs[g], st, sms);
+      launch_fast(w, L, hbs[g], st, sms, &marks);
       launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 2 : 0) + 1;
     }
   }
@@ -267,30 +292,57 @@ bool Engine::launch(cudaStream_t st) {
     L.segs = list(kLazySegs);
     L.n_segs = uint32_t(lists[kLazySegs].size());
     L.counter = counters + 2;
-    launches += launch_lazy(w, L, st, sms);
+    launches += launch_lazy(w, L, st, sms, &marks);
   }
   launch_plan(w, st);
+  marks.mark(kPhPlan, st);
   launches += 2;
   launch_join(w, counters + 3, st, sms);
+  marks.mark(kPhJoin, st);
   launches += w.npieces ? 1 : 0;
-  if (w.nck) {
+  bool framed = false;
+  for (const Stream& s : streams) framed |= s.fmt != kFmtRaw;
+  if (framed) {
     launch_checksums(w, st);
-    launches += 2;
+    launches += (w.nck ? 1 : 0) + 1;
   }
+  marks.mark(kPhCheck, st);
   launch_frame(w, st);
+  marks.mark(kPhFrame, st);
   launches += 1;
   CK(cudaGetLastError());
   return true;
 }
 
+// Milliseconds per phase of the last launch (after the stream completed).
+void Engine::phase_ms(float* ms) const {
+  for (int i = 0; i < kNumPhases; ++i) ms[i] = 0.f;
+  for (int i = 1; i < marks.n; ++i) {
+    float x = 0.f;
+    if (cudaEventElapsedTime(&x, marks.ev[i - 1], marks.ev[i]) == cudaSuccess && marks.id[i] >= 0)
+      ms[marks.id[i]] += x;
+  }
+}
+
 bool Engine::ensure_io(uint64_t in_bytes, uint64_t out_bytes) {
-  return d_in.ensure(in_bytes + 64) && d_out.ensure(out_bytes + 64);
+  // 256 bytes of padding: kernels read whole words (and a staged window of
+  // 64 bytes) past the last byte of a buffer, never using those bytes.
+  return d_in.ensure(in_bytes + 256) && d_out.ensure(out_bytes + 256);
 }
 
 // Whole-buffer or pigz-style compression of one host buffer.
+// Worst case of a pigz stream: every chunk stored (5 bytes per 65535-byte
+// piece) plus up to one byte of padding before each stored block.
+size_t parallel_bound(size_t n, int fmt, int level, size_t block) {
+  const size_t blk = block ? block : default_block(level);
+  const size_t nchunk = n ? (n + blk - 1) / blk : 1;
+  const size_t pieces = (blk + 65534) / 65535;
+  return std::max(framed_bound(n, fmt), n + nchunk * (5 * pieces + 1) + 32);
+}
+
 size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel,
                              size_t block) {
-  const size_t bound = framed_bound(n, fmt);
+  const size_t bound = parallel ? parallel_bound(n, fmt, level, block) : framed_bound(n, fmt);
   if (!ensure_io(align_up(n, 16), align_up(bound, 16))) return 0;
   if (n) {
     if (!h_stage.ensure(n)) return 0;

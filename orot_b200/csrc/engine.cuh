@@ -51,7 +51,9 @@ struct Segment {
   uint32_t tile_first, tile_count;
   uint32_t flags;
   int32_t level;       // clamped 0..12
-  // dynamic blocks (levels 4+): header bits and end-of-block code
+  // levels 4+: code table (288 litlen + 32 distance entries, code | len << 16),
+  // header bits (HLIT..code lengths) and end-of-block code
+  uint64_t codes;      // scratch byte offset of the code table
   uint64_t hdr_off;    // scratch byte offset of the HLIT..code-lengths bits
   uint32_t hdr_bits;
   uint32_t eob;        // EOB code | (code length << 16)
@@ -79,11 +81,17 @@ struct Tile {
   uint64_t rec;        // byte offset of WinRec[] (tiles with index > 0)
   uint64_t carry;      // byte offset of the carried-in hash table (index > 0)
   uint64_t slot;       // byte offset of this tile's published table (index < count-1)
+  uint64_t cand;       // levels 1-3, index > 0: u16 per position, candidate distance
+                       // that passed the first-byte check (0 = literal)
+  uint64_t tok;        // levels 4+: token word per position (0 = not a match start)
+  uint64_t hist;       // levels 4+: 320-bin literal/length + distance histogram
   // speculative walk (entry = tile start)
   uint32_t spec_bits, spec_matches, spec_exit, spec_tokens;
   // resolved parse: piece A = fix-up bits [0, fix_bits) from the fix-up
   // buffer, piece B = speculative bits [splice_bit, spec_bits)
   uint32_t fix_bits, splice_bit, fin_matches, fin_exit;
+  uint32_t fix_entry;  // parse entry the fix-up assumed
+  uint32_t pad1;
 };
 
 // A bit-range copy for the join kernel.  src == nullptr means "write the
@@ -117,5 +125,16 @@ __host__ __device__ inline uint64_t align_up(uint64_t v, uint64_t a) { return (v
 // most 9 bits and a match at most 25 bits per 3 covered bytes, so 9 bits per
 // input byte plus one match (31 bits) hanging over the tile end.
 __host__ __device__ inline uint64_t tile_stream_bytes(uint32_t tile_len) { return align_up(uint64_t(tile_len) * 9 / 8 + 64, 128); }
+
+// Levels 4+ use dynamic codes of up to 15 bits: a literal costs at most 15
+// bits and a match at most 48 bits per 3 covered bytes (16 bits per byte).
+__host__ __device__ inline uint64_t lazy_stream_bytes(uint32_t tile_len) { return align_up(uint64_t(tile_len) * 2 + 256, 128); }
+
+// Levels 4+: tiles of 32 x 258 bytes, each searching a 32 KiB window before
+// it.  A multiple of the longest match keeps runs of 258-byte matches (zero
+// fill, short periods) aligned with tile boundaries, so cutting the input
+// into independent tiles costs no extra token on such data.
+constexpr uint32_t kLazyTile = 32 * 258;
+constexpr uint32_t kLazyWindow = 32768;
 
 }  // namespace orotb

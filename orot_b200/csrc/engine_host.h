@@ -15,6 +15,7 @@ void set_error(const std::string& e);
 size_t raw_bound(size_t n);
 size_t framed_bound(size_t n, int fmt);
 size_t default_block(int level);
+size_t parallel_bound(size_t n, int fmt, int level, size_t block);
 int clamp_level(int l);
 
 struct DevBuf {
@@ -82,6 +83,9 @@ class Engine {
   uint64_t off_streams = 0, off_segs = 0, off_tiles = 0, off_ck = 0, off_pieces = 0, off_counters = 0;
   uint64_t off_lists[kNumLists] = {};
   int launches = 0;
+  Marks marks;
+  bool made_events = false;
+  void phase_ms(float* ms) const;
 };
 
 std::mutex& global_mutex();

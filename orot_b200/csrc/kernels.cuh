@@ -41,8 +41,23 @@ struct LazyLists {
   uint32_t* counter;
 };
 
-void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms);
-int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms);
+// Optional per-phase CUDA events: mark(id) records an event after phase id.
+enum Phase { kPhPre = 0, kPhWalk, kPhFix, kPhLazyLz, kPhLazyHuff, kPhLazyEnc, kPhPlan, kPhJoin, kPhCheck, kPhFrame,
+             kNumPhases };
+struct Marks {
+  cudaEvent_t ev[kNumPhases + 1];
+  int id[kNumPhases + 1];
+  int n = 0;
+  bool on = false;
+  void mark(int phase, cudaStream_t st) {
+    if (!on || n > kNumPhases) return;
+    cudaEventRecord(ev[n], st);
+    id[n++] = phase;
+  }
+};
+
+void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms, Marks* mk);
+int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms, Marks* mk);
 void launch_plan(const Work& wk, cudaStream_t st);
 void launch_checksums(const Work& wk, cudaStream_t st);
 void launch_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total, uint32_t init, int adler, uint32_t* res,

@@ -166,9 +166,12 @@ __global__ void __launch_bounds__(256) k_ck_block(Work wk, CrcPowers pw) {
   const uint8_t* p = wk.in + b.in_off + o0;
   uint32_t crc = 0, A = 0, B = 0;
   uint32_t i = 0;
-  const uint32_t* pw4 = reinterpret_cast<const uint32_t*>(p);
+  // aligned words, funnel-shifted when the block does not start on a word
+  const uint64_t ab = b.in_off + o0;
+  const uint32_t* pw4 = reinterpret_cast<const uint32_t*>(wk.in + (ab & ~uint64_t(3)));
+  const uint32_t sh = uint32_t(ab & 3) * 8;
   for (; i + 4 <= len; i += 4) {
-    const uint32_t v = __ldg(pw4 + (i >> 2));
+    const uint32_t v = sh ? __funnelshift_r(__ldg(pw4 + (i >> 2)), __ldg(pw4 + (i >> 2) + 1), sh) : __ldg(pw4 + (i >> 2));
     crc ^= v;
     crc = tb[3][crc & 0xFF] ^ tb[2][(crc >> 8) & 0xFF] ^ tb[1][(crc >> 16) & 0xFF] ^ tb[0][crc >> 24];
 #pragma unroll
@@ -359,10 +362,9 @@ void launch_plan(const Work& wk, cudaStream_t st) {
 }
 
 void launch_checksums(const Work& wk, cudaStream_t st) {
-  if (!wk.nck) return;
   const CrcPowers pw = host_crc_powers();
-  k_ck_block<<<wk.nck, 256, 0, st>>>(wk, pw);
-  k_ck_fold<<<(wk.nstreams + 127) / 128, 128, 0, st>>>(wk, pw);
+  if (wk.nck) k_ck_block<<<wk.nck, 256, 0, st>>>(wk, pw);
+  if (wk.nstreams) k_ck_fold<<<(wk.nstreams + 127) / 128, 128, 0, st>>>(wk, pw);
 }
 
 void launch_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total, uint32_t init, int adler, uint32_t* res,

@@ -68,181 +68,248 @@ __global__ void __launch_bounds__(256) k_lastocc(Work wk, const uint32_t* __rest
 template <int HB>
 __global__ void __launch_bounds__(256) k_carry_scan(Work wk, const uint32_t* __restrict__ seglist, uint32_t nseg) {
   constexpr int H = 1 << HB;
-  const uint32_t si = blockIdx.y;
-  if (si >= nseg) return;
-  const Segment sg = wk.segs[seglist[si]];
   const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= uint32_t(H)) return;
-  uint32_t run = 0;
-  for (uint32_t k = 0; k + 1 < sg.tile_count; ++k) {
-    uint32_t* slot = reinterpret_cast<uint32_t*>(wk.scratch + wk.tiles[sg.tile_first + k].slot);
-    run = max(run, slot[h]);
-    slot[h] = run;
+  for (uint32_t si = blockIdx.y; si < nseg; si += gridDim.y) {
+    const Segment sg = wk.segs[seglist[si]];
+    uint32_t run = 0;
+    for (uint32_t k = 0; k + 1 < sg.tile_count; ++k) {
+      uint32_t* slot = reinterpret_cast<uint32_t*>(wk.scratch + wk.tiles[sg.tile_first + k].slot);
+      run = max(run, slot[h]);
+      slot[h] = run;
+    }
   }
 }
 
 // ---------------------------------------------------------------- the walker
-struct WalkIn {
-  SegBytes sb;
-  uint32_t n;            // segment length
-  uint32_t ts, tl;       // tile start (segment-relative) and length
-  uint32_t entry;        // parse start, segment-relative, in [ts, ts+tl)
-  const uint32_t* carry; // head[] at tile start, nullptr = empty
-  uint32_t* out;         // bit-stream words
-  WinRec* rec_out;       // speculative walk: per-window records (may be null)
-  const WinRec* rec_in;  // fix-up walk: the speculative records
-};
-struct WalkOut {
-  uint32_t bits, matches, tokens, exit;
-  uint32_t merged, merge_win;
+// Per-warp shared state: head[] (walk only), the bit ring, and the staged
+// bytes of the current window (16 words starting at the word that holds the
+// window's first byte: positions wpos .. wpos+35 and the next window's
+// prefix).
+constexpr uint32_t kRing = 128, kWbuf = 16;
+
+struct WinState {
+  uint32_t np, cursor, flushed, matches, tokens;
 };
 
+// Stages 16 words of segment bytes starting at position wpos (rounded down to
+// a word) into wbuf; returns the byte offset of wpos inside wbuf.
+__device__ __forceinline__ uint32_t stage_window(const SegBytes& sb, uint32_t wpos, uint32_t* wbuf, uint32_t lane,
+                                                 uint32_t pre) {
+  if (lane < kWbuf) wbuf[lane] = pre;
+  __syncwarp();
+  return (wpos + sb.boff) & 3;
+}
+__device__ __forceinline__ uint32_t prefetch_window(const SegBytes& sb, uint32_t wpos, uint32_t lane) {
+  return lane < kWbuf ? __ldg(sb.w + ((wpos + sb.boff) >> 2) + lane) : 0u;
+}
+__device__ __forceinline__ uint32_t wload4(const uint32_t* wbuf, uint32_t off) {
+  return __funnelshift_r(wbuf[off >> 2], wbuf[(off >> 2) + 1], (off & 3) * 8);
+}
+
+// Capped common-prefix length of the bytes at p (staged at wbuf offset po)
+// and at q (global), at most cap <= 32.  The q-side words are loaded in one
+// batch so the lane pays one memory latency.
+__device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_t* wbuf, uint32_t po, uint32_t q,
+                                               uint32_t cap) {
+  const uint32_t qa = q + sb.boff;
+  const uint32_t* qw = sb.w + (qa >> 2);
+  const uint32_t qs = (qa & 3) * 8;
+  const uint32_t nw = (cap + 3 + (qa & 3)) / 4 + 1;  // words needed, <= 10
+  uint32_t v[10];
+#pragma unroll
+  for (int j = 0; j < 10; ++j) v[j] = (uint32_t(j) < nw) ? __ldg(qw + j) : 0u;
+  uint32_t n = 0;
+  bool open = true;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    if (open && n < cap) {
+      const uint32_t x = wload4(wbuf, po + 4 * j) ^ __funnelshift_r(v[j], v[j + 1], qs);
+      if (x) { n += (__ffs(x) - 1) >> 3; open = false; } else { n += 4; }
+    }
+  }
+  return n < cap ? n : cap;
+}
+
+// Greedy parse and fixed-Huffman emission of one 32-position window.  Lane
+// `lane` holds position wpos+lane; `d` is its candidate distance (0 = none).
+__device__ __forceinline__ void parse_window(const SegBytes& sb, uint32_t n, uint32_t wpos, uint32_t lim,
+                                             uint32_t lane, const uint32_t* wbuf, uint32_t woff, uint32_t d,
+                                             uint32_t* ring, uint32_t* out, WinState& st) {
+  const uint32_t p = wpos + lane;
+  uint32_t clen = 0;
+  bool exact = true;
+  if (d && p >= st.np && lane < lim) {
+    const uint32_t maxm = min(258u, n - p);
+    const uint32_t cap = min(maxm, max(3u, 32u - lane));
+    clen = lcp_window(sb, wbuf, woff + lane, p - d, cap);
+    exact = clen < cap || cap == maxm;
+    if (clen < 3) clen = 0;
+  }
+  const uint32_t M = __ballot_sync(kFull, clen >= 3);
+  const uint32_t limmask = lim == 32 ? kFull : ((1u << lim) - 1);
+  uint32_t cur = st.np - wpos, visited = 0;
+  int xl = -1;
+  while (cur < lim) {
+    const uint32_t nm = M & limmask & (kFull << cur);
+    if (!nm) { visited |= limmask & (kFull << cur); cur = lim; break; }
+    const uint32_t j = __ffs(nm) - 1;
+    visited |= (kFull << cur) & ((2u << j) - 1u);
+    const uint32_t lj = __shfl_sync(kFull, clen, j);
+    const bool ej = __shfl_sync(kFull, exact, j);
+    if (ej) { cur = j + lj; } else { xl = int(j); break; }
+  }
+  uint32_t full = 0;
+  if (xl >= 0) {
+    // warp-cooperative extension, 128 bytes per round
+    const uint32_t pj = wpos + xl;
+    const uint32_t dj = __shfl_sync(kFull, d, xl);
+    const uint32_t c0 = __shfl_sync(kFull, clen, xl);
+    const uint32_t maxm = min(258u, n - pj);
+    full = c0;
+    for (uint32_t base = c0; base < maxm; base += 128) {
+      const uint32_t off = base + 4 * lane;
+      uint32_t stop = kFull;
+      if (off < maxm) {
+        const uint32_t x = sb.load4(pj + off) ^ sb.load4(pj - dj + off);
+        const uint32_t m = x ? ((__ffs(x) - 1) >> 3) : 4u;
+        const uint32_t l4 = min(4u, maxm - off);
+        if (m < l4) stop = off + m;
+        else if (off + 4 >= maxm) stop = maxm;
+      }
+      const uint32_t b = __ballot_sync(kFull, stop != kFull);
+      if (b) { full = __shfl_sync(kFull, stop, __ffs(b) - 1); break; }
+    }
+    cur = uint32_t(xl) + full;
+  }
+  const bool vis = (visited >> lane) & 1u;
+  const bool ism = vis && ((M >> lane) & 1u);
+  uint32_t code = 0, nb = 0;
+  if (vis) {
+    if (ism) fixed_match(int(lane) == xl ? full : clen, d, code, nb);
+    else fixed_literal(wload4(wbuf, woff + lane) & 0xFFu, code, nb);
+  }
+  uint32_t incl = nb;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= uint32_t(o)) incl += t;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  if (nb) {
+    const uint32_t bp = st.cursor + incl - nb, wd = bp >> 5, sh = bp & 31;
+    atomicOr(&ring[wd & (kRing - 1)], code << sh);
+    if (sh + nb > 32) atomicOr(&ring[(wd + 1) & (kRing - 1)], code >> (32 - sh));
+  }
+  st.cursor += total;
+  st.tokens += __popc(visited);
+  st.matches += __popc(visited & M);
+  st.np = wpos + cur;
+  __syncwarp();
+  while ((st.cursor >> 5) >= st.flushed + 32) {
+    out[st.flushed + lane] = ring[(st.flushed + lane) & (kRing - 1)];
+    ring[(st.flushed + lane) & (kRing - 1)] = 0;
+    st.flushed += 32;
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void flush_tail(uint32_t* ring, uint32_t* out, const WinState& st, uint32_t lane) {
+  const uint32_t nwords = (st.cursor + 31) >> 5;
+  for (uint32_t i = st.flushed + lane; i < nwords; i += 32) out[i] = ring[i & (kRing - 1)];
+  __syncwarp();
+}
+
+struct TileView {
+  SegBytes sb;
+  uint32_t n, ts, tl;
+};
+
+__device__ __forceinline__ TileView tile_view(const Work& wk, const Tile& t, const Segment& sg) {
+  const uint64_t o = sg.in_off;
+  return TileView{SegBytes{reinterpret_cast<const uint32_t*>(wk.in + (o & ~uint64_t(3))), uint32_t(o & 3)}, sg.len,
+                  t.start, t.len};
+}
+
+// Speculative walk of one tile (parse entry = tile start): inserts every
+// position into head[], records the candidate distance of every position and
+// the parse entry of every window, emits the fixed-Huffman bits.
 template <int HB>
-__device__ WalkOut walk_tile(const WalkIn& a, uint32_t* __restrict__ head, uint32_t* __restrict__ ring) {
+__device__ WinState walk_tile(const TileView& tv, const uint32_t* carry, uint32_t* head, uint32_t* ring,
+                              uint32_t* wbuf, uint32_t* out, WinRec* rec, uint16_t* cand16) {
   constexpr int H = 1 << HB;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1;
-  if (a.carry) {
-    for (int i = lane; i < H; i += 32) head[i] = __ldg(a.carry + i);
+  if (carry) {
+    for (int i = lane; i < H; i += 32) head[i] = __ldg(carry + i);
   } else {
     for (int i = lane; i < H; i += 32) head[i] = 0;
   }
-  for (int i = lane; i < 128; i += 32) ring[i] = 0;
+  for (uint32_t i = lane; i < kRing; i += 32) ring[i] = 0;
   __syncwarp();
-
-  WalkOut r{};
-  uint32_t np = a.entry, cursor = 0, flushed = 0, matches = 0, tokens = 0;
-  const uint32_t tend = a.ts + a.tl;
-  const uint32_t nwin = (a.tl + 31) >> 5;
+  WinState st{tv.ts, 0, 0, 0, 0};
+  const uint32_t tend = tv.ts + tv.tl;
+  const uint32_t nwin = (tv.tl + 31) >> 5;
+  uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
   for (uint32_t w = 0; w < nwin; ++w) {
-    const uint32_t wpos = a.ts + (w << 5);
-    if (a.rec_in) {
-      const uint32_t se = a.ts + a.rec_in[w].entry;
-      if (np == se) { r.merged = 1; r.merge_win = w; break; }
-    }
-    if (a.rec_out && lane == 0) a.rec_out[w] = WinRec{np - a.ts, cursor, matches, tokens};
-
-    // -- insert the 32 positions of this window into head[]
+    const uint32_t wpos = tv.ts + (w << 5);
+    const uint32_t woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
+    if (w + 1 < nwin) pre = prefetch_window(tv.sb, wpos + 32, lane);
+    if (rec && lane == 0) rec[w] = WinRec{st.np - tv.ts, st.cursor, st.matches, st.tokens};
     const uint32_t p = wpos + lane;
-    const bool in_tile = p < tend;
-    const bool ins = in_tile && p + 4 <= a.n;
-    uint32_t v4 = 0, h = kFull;
-    if (ins) { v4 = a.sb.load4(p); h = hash_fast(v4, HB); }
+    const bool ins = p < tend && p + 4 <= tv.n;
+    const uint32_t v4 = wload4(wbuf, woff + lane);
+    const uint32_t h = ins ? hash_fast(v4, HB) : kFull;
     const uint32_t peers = __match_any_sync(kFull, h);
     const uint32_t before = peers & lt;
     uint32_t cand = 0;
     if (ins) cand = before ? (wpos + 31 - __clz(before)) : head[h];
     __syncwarp();
     if (ins && (peers >> lane) == 1u) head[h] = p;
+    // candidate distance after the first-byte check at the candidate itself
+    uint32_t d = 0;
+    if (ins && cand != 0) {
+      const uint32_t dist = (p - cand) & 0x7FFFu;
+      if (dist != 0 && tv.sb.byte(cand) == (v4 & 0xFFu)) d = dist;
+    }
+    if (cand16 && p < tend) cand16[p - tv.ts] = uint16_t(d);
     __syncwarp();
-
-    // -- greedy parse over the window
     const uint32_t lim = min(32u, tend - wpos);
-    if (np >= wpos + lim) continue;
-    uint32_t clen = 0, dist = 0;
-    bool exact = true;
-    if (ins && p >= np && cand != 0) {
-      dist = (p - cand) & 0x7FFFu;
-      if (dist != 0 && a.sb.byte(cand) == (v4 & 0xFFu)) {
-        const uint32_t maxm = min(258u, a.n - p);
-        const uint32_t cap = min(maxm, max(3u, 32u - lane));
-        clen = lcp_capped(a.sb, p, p - dist, cap);
-        exact = clen < cap || cap == maxm;
-        if (clen < 3) clen = 0;
-      }
-    }
-    const uint32_t M = __ballot_sync(kFull, clen >= 3);
-    const uint32_t limmask = lim == 32 ? kFull : ((1u << lim) - 1);
-    uint32_t cur = np - wpos, visited = 0;
-    int xl = -1;  // lane whose match runs past the window and needs its full length
-    while (cur < lim) {
-      const uint32_t nm = M & limmask & (kFull << cur);
-      if (!nm) { visited |= limmask & (kFull << cur); cur = lim; break; }
-      const uint32_t j = __ffs(nm) - 1;
-      visited |= (kFull << cur) & ((2u << j) - 1u);
-      const uint32_t lj = __shfl_sync(kFull, clen, j);
-      const bool ej = __shfl_sync(kFull, exact, j);
-      if (ej) { cur = j + lj; } else { xl = int(j); break; }
-    }
-    uint32_t full = 0;
-    if (xl >= 0) {
-      // warp-cooperative extension, 128 bytes per round
-      const uint32_t pj = wpos + xl;
-      const uint32_t dj = __shfl_sync(kFull, dist, xl);
-      const uint32_t c0 = __shfl_sync(kFull, clen, xl);
-      const uint32_t maxm = min(258u, a.n - pj);
-      full = c0;
-      for (uint32_t base = c0; base < maxm; base += 128) {
-        const uint32_t off = base + 4 * lane;
-        uint32_t stop = kFull;
-        if (off < maxm) {
-          const uint32_t x = a.sb.load4(pj + off) ^ a.sb.load4(pj - dj + off);
-          const uint32_t m = x ? ((__ffs(x) - 1) >> 3) : 4u;
-          const uint32_t l4 = min(4u, maxm - off);
-          if (m < l4) stop = off + m;
-          else if (off + 4 >= maxm) stop = maxm;
-        }
-        const uint32_t b = __ballot_sync(kFull, stop != kFull);
-        if (b) { full = __shfl_sync(kFull, stop, __ffs(b) - 1); break; }
-      }
-      cur = uint32_t(xl) + full;
-    }
-
-    // -- emit the visited tokens
-    const bool vis = (visited >> lane) & 1u;
-    const bool ism = vis && ((M >> lane) & 1u);
-    uint32_t code = 0, nb = 0;
-    if (vis) {
-      if (ism) fixed_match(int(lane) == xl ? full : clen, dist, code, nb);
-      else fixed_literal(ins ? (v4 & 0xFFu) : a.sb.byte(p), code, nb);
-    }
-    uint32_t incl = nb;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(kFull, incl, o);
-      if (lane >= uint32_t(o)) incl += t;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    if (nb) {
-      const uint32_t bp = cursor + incl - nb, wd = bp >> 5, sh = bp & 31;
-      atomicOr(&ring[wd & 127], code << sh);
-      if (sh + nb > 32) atomicOr(&ring[(wd + 1) & 127], code >> (32 - sh));
-    }
-    cursor += total;
-    tokens += __popc(visited);
-    matches += __popc(visited & M);
-    np = wpos + cur;
-    __syncwarp();
-    while ((cursor >> 5) >= flushed + 32) {
-      a.out[flushed + lane] = ring[(flushed + lane) & 127];
-      ring[(flushed + lane) & 127] = 0;
-      flushed += 32;
-      __syncwarp();
-    }
+    if (st.np < wpos + lim) parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st);
   }
-  const uint32_t nwords = (cursor + 31) >> 5;
-  for (uint32_t i = flushed + lane; i < nwords; i += 32) a.out[i] = ring[i & 127];
-  __syncwarp();
-  r.bits = cursor;
-  r.matches = matches;
-  r.tokens = tokens;
-  r.exit = np;
-  return r;
+  flush_tail(ring, out, st, lane);
+  return st;
 }
 
-__device__ __forceinline__ WalkIn walk_args(const Work& wk, const Tile& t, const Segment& sg) {
-  WalkIn a;
-  const uint64_t o = sg.in_off;
-  a.sb = SegBytes{reinterpret_cast<const uint32_t*>(wk.in + (o & ~uint64_t(3))), uint32_t(o & 3)};
-  a.n = sg.len;
-  a.ts = t.start;
-  a.tl = t.len;
-  a.entry = t.start;
-  a.carry = t.index ? reinterpret_cast<const uint32_t*>(wk.scratch + t.carry) : nullptr;
-  a.out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch);
-  a.rec_out = nullptr;
-  a.rec_in = nullptr;
-  return a;
+// Re-parse of one tile from `entry` using the recorded candidate distances,
+// until the parse meets the speculative one at a window boundary.
+struct FixOut {
+  uint32_t bits, matches, exit, merged, merge_win;
+};
+__device__ FixOut fix_tile(const TileView& tv, uint32_t entry, const WinRec* rec, const uint16_t* cand16,
+                           uint32_t* ring, uint32_t* wbuf, uint32_t* out) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t i = lane; i < kRing; i += 32) ring[i] = 0;
+  __syncwarp();
+  WinState st{entry, 0, 0, 0, 0};
+  FixOut r{};
+  const uint32_t tend = tv.ts + tv.tl;
+  const uint32_t nwin = (tv.tl + 31) >> 5;
+  for (uint32_t w = (entry - tv.ts) >> 5; w < nwin; ++w) {
+    const uint32_t wpos = tv.ts + (w << 5);
+    if (st.np == tv.ts + rec[w].entry) { r.merged = 1; r.merge_win = w; break; }
+    const uint32_t lim = min(32u, tend - wpos);
+    if (st.np >= wpos + lim) continue;
+    const uint32_t pre = prefetch_window(tv.sb, wpos, lane);
+    const uint32_t woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
+    const uint32_t d = lane < lim ? cand16[(w << 5) + lane] : 0u;
+    parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st);
+  }
+  flush_tail(ring, out, st, lane);
+  r.bits = st.cursor;
+  r.matches = st.matches;
+  r.exit = st.np;
+  return r;
 }
 
 // ---------------------------------------------------------------- k_walk
@@ -252,8 +319,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_walk(Work wk, const uint32_t* __
   extern __shared__ uint32_t sm[];
   constexpr int H = 1 << HB;
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* head = sm + wid * (H + 128);
+  uint32_t* head = sm + wid * (H + kRing + kWbuf);
   uint32_t* ring = head + H;
+  uint32_t* wbuf = ring + kRing;
   for (;;) {
     uint32_t i = 0;
     if (lane == 0) i = atomicAdd(counter, 1u);
@@ -262,72 +330,104 @@ __global__ void __launch_bounds__(WARPS * 32) k_walk(Work wk, const uint32_t* __
     Tile* tp = wk.tiles + list[i];
     const Tile t = *tp;
     const Segment sg = wk.segs[t.seg];
-    WalkIn a = walk_args(wk, t, sg);
-    if (t.index) a.rec_out = reinterpret_cast<WinRec*>(wk.scratch + t.rec);
-    const WalkOut r = walk_tile<HB>(a, head, ring);
+    const TileView tv = tile_view(wk, t, sg);
+    const uint32_t* carry = t.index ? reinterpret_cast<const uint32_t*>(wk.scratch + t.carry) : nullptr;
+    WinRec* rec = t.index ? reinterpret_cast<WinRec*>(wk.scratch + t.rec) : nullptr;
+    uint16_t* c16 = t.index ? reinterpret_cast<uint16_t*>(wk.scratch + t.cand) : nullptr;
+    uint32_t* out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch);
+    const WinState r = walk_tile<HB>(tv, carry, head, ring, wbuf, out, rec, c16);
     if (lane == 0) {
-      tp->spec_bits = r.bits;
+      tp->spec_bits = r.cursor;
       tp->spec_matches = r.matches;
-      tp->spec_exit = r.exit;
+      tp->spec_exit = r.np;
       tp->spec_tokens = r.tokens;
       tp->fix_bits = 0;
       tp->splice_bit = 0;
       tp->fin_matches = r.matches;
-      tp->fin_exit = r.exit;
+      tp->fin_exit = r.np;
+      tp->fix_entry = t.start;
     }
   }
 }
 
-// ---------------------------------------------------------------- k_fixup
-template <int HB, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_fixup(Work wk, const uint32_t* __restrict__ seglist, uint32_t nseg) {
-  extern __shared__ uint32_t sm[];
-  constexpr int H = 1 << HB;
+// ---------------------------------------------------------------- fix-up
+// Applies the re-parse of tile t from `entry` and returns its true exit.
+__device__ uint32_t fix_apply(const Work& wk, Tile* tp, uint32_t entry, uint32_t* ring, uint32_t* wbuf) {
+  const Tile t = *tp;
+  const Segment sg = wk.segs[t.seg];
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t fix_bits = 0, splice = 0, fin_m = t.spec_matches, fin_x = t.spec_exit;
+  if (entry >= t.start + t.len) {  // a match of the previous tile covers this one
+    splice = t.spec_bits;
+    fin_m = 0;
+    fin_x = entry;
+  } else if (entry != t.start) {
+    const TileView tv = tile_view(wk, t, sg);
+    const WinRec* rec = reinterpret_cast<const WinRec*>(wk.scratch + t.rec);
+    const uint16_t* c16 = reinterpret_cast<const uint16_t*>(wk.scratch + t.cand);
+    uint32_t* out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch + tile_stream_bytes(t.len));
+    const FixOut r = fix_tile(tv, entry, rec, c16, ring, wbuf, out);
+    fix_bits = r.bits;
+    if (r.merged) {
+      const WinRec rc = rec[r.merge_win];
+      splice = rc.bit;
+      fin_m = r.matches + (t.spec_matches - rc.matches);
+      fin_x = t.spec_exit;
+    } else {
+      splice = t.spec_bits;
+      fin_m = r.matches;
+      fin_x = r.exit;
+    }
+  }
+  if (lane == 0) {
+    tp->fix_bits = fix_bits;
+    tp->splice_bit = splice;
+    tp->fin_matches = fin_m;
+    tp->fin_exit = fin_x;
+    tp->fix_entry = entry;
+  }
+  __syncwarp();
+  return fin_x;
+}
+
+// Round 1: every tile after the first, in parallel, assuming the previous
+// tile's speculative parse was the true one.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_fix1(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
+                                                      uint32_t* __restrict__ counter) {
+  __shared__ uint32_t sm[WARPS][kRing + kWbuf];
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* head = sm + wid * (H + 128);
-  uint32_t* ring = head + H;
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(counter, 1u);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= nlist) break;
+    Tile* tp = wk.tiles + list[i];
+    if (tp->index == 0) continue;
+    fix_apply(wk, tp, tp[-1].spec_exit, sm[wid], sm[wid] + kRing);
+  }
+}
+
+// Round 2: per segment, in order; a tile is redone only when its
+// predecessor's true exit differs from the entry round 1 assumed.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_fix2(Work wk, const uint32_t* __restrict__ seglist, uint32_t nseg) {
+  __shared__ uint32_t sm[WARPS][kRing + kWbuf];
+  const uint32_t wid = threadIdx.x >> 5;
   const uint32_t si = blockIdx.x * WARPS + wid;
   if (si >= nseg) return;
   const Segment sg = wk.segs[seglist[si]];
   uint32_t exit = wk.tiles[sg.tile_first].fin_exit;
   for (uint32_t k = 1; k < sg.tile_count; ++k) {
     Tile* tp = wk.tiles + sg.tile_first + k;
-    const Tile t = *tp;
-    uint32_t fix_bits = 0, splice = 0, fin_m = t.spec_matches, fin_x = t.spec_exit;
-    if (exit >= t.start + t.len) {          // a match of the previous tile covers this one
-      splice = t.spec_bits; fin_m = 0; fin_x = exit;
-    } else if (exit != t.start) {
-      WalkIn a = walk_args(wk, t, sg);
-      a.entry = exit;
-      a.out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch + tile_stream_bytes(t.len));
-      a.rec_in = reinterpret_cast<const WinRec*>(wk.scratch + t.rec);
-      const WalkOut r = walk_tile<HB>(a, head, ring);
-      fix_bits = r.bits;
-      if (r.merged) {
-        const WinRec rc = a.rec_in[r.merge_win];
-        splice = rc.bit;
-        fin_m = r.matches + (t.spec_matches - rc.matches);
-        fin_x = t.spec_exit;
-      } else {
-        splice = t.spec_bits;
-        fin_m = r.matches;
-        fin_x = r.exit;
-      }
-    }
-    if (lane == 0) {
-      tp->fix_bits = fix_bits;
-      tp->splice_bit = splice;
-      tp->fin_matches = fin_m;
-      tp->fin_exit = fin_x;
-    }
-    exit = fin_x;
-    __syncwarp();
+    if (tp->fix_entry == exit) { exit = tp->fin_exit; continue; }
+    exit = fix_apply(wk, tp, exit, sm[wid], sm[wid] + kRing);
   }
 }
 
 // ---------------------------------------------------------------- launchers
 template <int HB>
-static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, int sms) {
+static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, int sms, Marks* mk) {
   constexpr int H = 1 << HB;
   constexpr int WARPS = HB <= 12 ? 4 : 1;
   const size_t tbl_bytes = size_t(H) * 4;
@@ -336,10 +436,11 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
     k_lastocc<HB><<<L.n_lastocc, 256, tbl_bytes, st>>>(wk, L.lastocc, L.n_lastocc);
   }
   if (L.n_multi) {
-    dim3 g((H + 255) / 256, L.n_multi);
+    dim3 g((H + 255) / 256, L.n_multi < 65535u ? L.n_multi : 65535u);
     k_carry_scan<HB><<<g, 256, 0, st>>>(wk, L.multi, L.n_multi);
   }
-  const size_t wsm = size_t(WARPS) * (H + 128) * 4;
+  mk->mark(kPhPre, st);
+  const size_t wsm = size_t(WARPS) * (H + kRing + kWbuf) * 4;
   if (L.n_walk) {
     cudaFuncSetAttribute(k_walk<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm));
     int per_sm = 0;
@@ -350,15 +451,21 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
     if (blocks > need) blocks = need;
     k_walk<HB, WARPS><<<blocks, WARPS * 32, wsm, st>>>(wk, L.walk, L.n_walk, L.counter);
   }
+  mk->mark(kPhWalk, st);
   if (L.n_multi) {
-    cudaFuncSetAttribute(k_fixup<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm));
-    k_fixup<HB, WARPS><<<(L.n_multi + WARPS - 1) / WARPS, WARPS * 32, wsm, st>>>(wk, L.multi, L.n_multi);
+    constexpr int FW = 8;
+    uint32_t blocks = uint32_t(sms) * 8;
+    const uint32_t need = (L.n_walk + FW - 1) / FW;
+    if (blocks > need) blocks = need;
+    k_fix1<FW><<<blocks, FW * 32, 0, st>>>(wk, L.walk, L.n_walk, L.counter + 4);
+    k_fix2<FW><<<(L.n_multi + FW - 1) / FW, FW * 32, 0, st>>>(wk, L.multi, L.n_multi);
   }
+  mk->mark(kPhFix, st);
 }
 
-void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms) {
-  if (hash_bits == 12) launch_fast_t<12>(wk, L, st, sms);
-  else launch_fast_t<14>(wk, L, st, sms);
+void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms, Marks* mk) {
+  if (hash_bits == 12) launch_fast_t<12>(wk, L, st, sms, mk);
+  else launch_fast_t<14>(wk, L, st, sms, mk);
 }
 
 }  // namespace orotb

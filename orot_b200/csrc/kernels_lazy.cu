@@ -1,6 +1,643 @@
 // kernels_lazy.cu -- LZ77 with hash chains and lazy evaluation (levels 4-12)
-// plus dynamic Huffman blocks.  (Work in progress: not wired yet.)
+// and dynamic Huffman blocks, on sm_100a.
+//
+// Search semantics follow the reference's standard path
+// (src/deflate/lz77.cpp:66-156, 435-495): chains of earlier positions with the
+// same 16-bit hash, newest first; up to max_chain members examined, a 4-byte
+// mismatch counts as a miss and miss_limit consecutive misses end the walk,
+// the longest match wins (ties keep the nearest), nice_len ends the walk;
+// the lazy step searches pos+1 with half the chain and needs two more bytes.
+// GPU-native differences, all keeping the stream valid:
+//   * a chain ends at the 32 KiB window edge (the reference keeps walking
+//     with distances taken mod 32768);
+//   * the input is cut into independent 8 KiB tiles: each tile parses from
+//     its own first byte and matches do not run past its end, while still
+//     referencing up to 32 KiB before the tile;
+//   * levels 10-12 use the same chains with 1024/2048/4096 steps and lazy
+//     depth 3 instead of the reference's binary tree;
+//   * code lengths come from an optimal two-queue Huffman construction with
+//     the ITU-T T.81 Annex K.3 length limiter, and the block type is chosen
+//     on exact sizes (the reference uses a flat header estimate).
+//
+//   k_lz     one CTA per tile: stage the window + tile in shared memory,
+//            link every position to the previous one with the same 15-bit
+//            hash, search every position (F: normal, G: lazy) in parallel,
+//            parse on one thread with a bitmap to skip literal runs, then a
+//            block-wide max-scan marks covered bytes and fills the histogram.
+//   k_huff   one warp per segment: code lengths, canonical codes, block type,
+//            RLE code-length header (deflate_block.cpp:196-290 rules).
+//   k_enc    one warp per tile: resolves tokens 32 positions at a time and
+//            packs the codes into the tile's bit buffer.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "engine.cuh"
+#include "deflate_device.cuh"
 #include "kernels.cuh"
+
 namespace orotb {
-int launch_lazy(const Work&, const LazyLists&, cudaStream_t, int) { return 0; }
+
+namespace {
+
+constexpr uint32_t kAll = 0xFFFFFFFFu;
+constexpr uint32_t T = kLazyTile, W = kLazyWindow;
+constexpr uint32_t kRegion = W + T;                 // positions with links
+constexpr uint32_t kDataBytes = 41472;             // >= W + T + 16 (align) + 16 (tail)
+constexpr uint32_t kLinkBytes = (kRegion * 2 + 127) / 128 * 128;  // u16 per position
+constexpr uint32_t kTblBytes = T * 8 > 65536 ? T * 8 : 65536;      // u16 x 2^15 table, later F[T] + G[T]
+constexpr uint32_t kFmWords = T / 32;
+static_assert(T % 32 == 0, "tiles are whole windows of 32 positions");
+constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFmWords * 4 + 320 * 4 + 64 * 4;
+static_assert(kDataBytes >= W + T + 32, "data area");
+static_assert(T * 8 <= kTblBytes, "F and G fit the table area");
+static_assert(T * 4 <= kLinkBytes, "token words fit the link area");
+
+struct LazyCfg { int chain, nice, lazy, miss; };
+__constant__ LazyCfg c_lazy[13] = {
+    {0, 0, 0, 5},       {0, 0, 0, 5},       {0, 0, 0, 5},       {0, 0, 0, 5},
+    {64, 128, 1, 5},    {128, 128, 1, 5},   {128, 258, 1, 5},   {256, 258, 2, 6},
+    {512, 258, 2, 6},   {768, 258, 3, 6},   {1024, 258, 3, 8},  {2048, 258, 3, 8},
+    {4096, 258, 3, 8}};
+
+struct SmemBytes {
+  const uint32_t* w;  // 16-byte aligned shared words
+  uint32_t boff;      // byte offset of region position 0
+  __device__ __forceinline__ uint32_t load4(uint32_t r) const {
+    const uint32_t i = r + boff;
+    return __funnelshift_r(w[i >> 2], w[(i >> 2) + 1], (i & 3) * 8);
+  }
+  __device__ __forceinline__ uint32_t byte(uint32_t r) const {
+    const uint32_t i = r + boff;
+    return (w[i >> 2] >> ((i & 3) * 8)) & 0xFFu;
+  }
+};
+
+__device__ __forceinline__ uint32_t hash16(uint32_t v) { return (v * 0x9E3779B1u) >> 16; }
+__device__ __forceinline__ uint32_t hash15(uint32_t v) { return (v * 0x9E3779B1u) >> 17; }
+
+// Chain search at region position r; returns len << 16 | dist or 0.
+__device__ uint32_t lz_search(const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t r, uint32_t excl,
+                              uint32_t maxm, int chain, int nice, int miss_limit, uint32_t v4p) {
+  const uint32_t h16p = hash16(v4p);
+  uint32_t best = 2, bd = 0, q = r;
+  int steps = chain, misses = 0, budget = 2 * chain + 64;
+  while (budget-- > 0) {
+    const uint32_t l = link[q];
+    if (!l) break;
+    q -= l;
+    if (r - q > 32767u) break;
+    if (q == excl) continue;
+    const uint32_t v = sd.load4(q);
+    if (v != v4p && hash16(v) != h16p) continue;  // same 15-bit bucket, other 16-bit chain
+    if (steps == 0) break;
+    --steps;
+    if (v != v4p) {
+      if (++misses >= miss_limit) break;
+      continue;
+    }
+    misses = 0;
+    uint32_t len = 4;
+    while (len < maxm) {
+      const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
+      if (x) { len += (__ffs(x) - 1) >> 3; break; }
+      len += 4;
+    }
+    if (len > maxm) len = maxm;
+    if (len > best) {
+      best = len;
+      bd = r - q;
+      if (int(len) >= nice) break;
+    }
+  }
+  return best >= 3 ? (best << 16) | bd : 0u;
+}
+
+__device__ __forceinline__ uint32_t block_max_excl(uint32_t v, uint32_t* scan) {
+  const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kAll, inc, o);
+    if (lane >= uint32_t(o)) inc = max(inc, t);
+  }
+  if (lane == 31) scan[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t x = lane < (blockDim.x >> 5) ? scan[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kAll, x, o);
+      if (lane >= uint32_t(o)) x = max(x, t);
+    }
+    scan[32 + lane] = x;  // inclusive over warps
+  }
+  __syncthreads();
+  const uint32_t before_warp = wid ? scan[32 + wid - 1] : 0;
+  const uint32_t excl_lane = __shfl_up_sync(kAll, inc, 1);
+  return max(before_warp, lane ? excl_lane : 0u);
+}
+
+__device__ __forceinline__ uint32_t len_sym(uint32_t len) {
+  uint32_t li, ne, ev;
+  length_code(len, li, ne, ev);
+  return li;
+}
+__device__ __forceinline__ uint32_t dist_sym(uint32_t d) {
+  uint32_t dc, ne, ev;
+  dist_code(d, dc, ne, ev);
+  return dc;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- k_lz
+__global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restrict__ list, uint32_t nlist) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  uint32_t* sdata = reinterpret_cast<uint32_t*>(sm);
+  uint16_t* link = reinterpret_cast<uint16_t*>(sm + kDataBytes);
+  uint16_t* tbl = reinterpret_cast<uint16_t*>(sm + kDataBytes + kLinkBytes);
+  uint32_t* F = reinterpret_cast<uint32_t*>(sm + kDataBytes + kLinkBytes);
+  uint32_t* G = F + T;
+  uint32_t* fm = reinterpret_cast<uint32_t*>(sm + kDataBytes + kLinkBytes + kTblBytes);
+  uint32_t* hist = fm + kFmWords;
+  uint32_t* scan = hist + 320;
+  uint32_t* tok_s = reinterpret_cast<uint32_t*>(link);  // after the searches
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+  if (blockIdx.x >= nlist) return;
+  Tile* tp = wk.tiles + list[blockIdx.x];
+  const Tile t = *tp;
+  const Segment sg = wk.segs[t.seg];
+  const LazyCfg cfg = c_lazy[sg.level];
+  const uint32_t ts = t.start, tl = t.len, tend = ts + tl;
+  const uint32_t rs = ts > W ? ts - W : 0;           // region start (segment-relative)
+  const uint32_t nreg = tend - rs;                    // positions with links
+  const uint32_t copy_end = min(sg.len, tend + 8);    // bytes staged
+  // -- stage bytes [rs, copy_end) at 16-byte granularity
+  const uint64_t g0 = (sg.in_off + rs) & ~uint64_t(15);
+  const uint32_t boff = uint32_t(sg.in_off + rs - g0);
+  const uint32_t n16 = (boff + (copy_end - rs) + 15) / 16;
+  const uint4* src = reinterpret_cast<const uint4*>(wk.in + g0);
+  uint4* dst = reinterpret_cast<uint4*>(sm);
+  for (uint32_t i = tid; i < kDataBytes / 16; i += blockDim.x)
+    dst[i] = i < n16 ? __ldg(src + i) : make_uint4(0, 0, 0, 0);
+  for (uint32_t i = tid; i < kTblBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(tbl)[i] = kAll;
+  for (uint32_t i = tid; i < 320; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const SmemBytes sd{sdata, boff};
+
+  // -- links: previous position with the same 15-bit hash (warp 0, in order)
+  if (wid == 0) {
+    const uint32_t lt = (1u << lane) - 1;
+    for (uint32_t base = 0; base < nreg; base += 32) {
+      const uint32_t x = base + lane;
+      const bool valid = x < nreg && rs + x + 4 <= sg.len;
+      const uint32_t h = valid ? hash15(sd.load4(x)) : kAll;
+      const uint32_t peers = __match_any_sync(kAll, h);
+      const uint32_t before = peers & lt;
+      uint32_t l = 0;
+      if (valid) {
+        const uint32_t pred = before ? base + 31 - __clz(before) : tbl[h];
+        l = pred == 0xFFFFu ? 0u : x - pred;
+      }
+      if (x < nreg) link[x] = uint16_t(l);
+      __syncwarp();
+      if (valid && (peers >> lane) == 1u) tbl[h] = uint16_t(x);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+
+  // -- searches at every tile position (whole warps per iteration: T is a
+  // multiple of 32)
+  const uint32_t lazy_chain = cfg.chain > 1 ? uint32_t(cfg.chain) >> 1 : 1u;
+  for (uint32_t i = tid; i < T; i += blockDim.x) {
+    uint32_t f = 0, g = 0;
+    if (i < tl && i + 4 <= tl) {
+      const uint32_t r = ts - rs + i;
+      const uint32_t v = sd.load4(r);
+      const uint32_t maxm = min(258u, tl - i);
+      f = lz_search(sd, link, r, kAll, maxm, cfg.chain, cfg.nice, cfg.miss, v);
+      if (cfg.lazy) g = lz_search(sd, link, r, r - 1, maxm, int(lazy_chain), cfg.nice, cfg.miss, v);
+    }
+    F[i] = f;
+    G[i] = g;
+    const uint32_t b = __ballot_sync(kAll, f != 0);
+    if (lane == 0) fm[i >> 5] = b;
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
+  __syncthreads();
+
+  // -- parse (reference lazy rule, lz77.cpp:449-493, with n = tile end)
+  if (tid == 0) {
+    uint32_t i = 0, nm = 0;
+    while (i < tl) {
+      if (!((fm[i >> 5] >> (i & 31)) & 1u)) {
+        uint32_t w = i >> 5;
+        uint32_t bits = fm[w] & (kAll << (i & 31));
+        while (!bits && ++w < kFmWords) bits = fm[w];
+        if (!bits) break;
+        i = w * 32 + __ffs(bits) - 1;
+        if (i >= tl) break;
+      }
+      uint32_t bl = F[i] >> 16, bd = F[i] & 0xFFFFu;
+      int k = cfg.lazy;
+      while (k > 0 && i + bl + 1 < tl && i + 4 <= tl) {
+        const uint32_t g = G[i + 1];
+        if ((g >> 16) > bl + 1) {
+          ++i;
+          bl = g >> 16;
+          bd = g & 0xFFFFu;
+          --k;
+        } else {
+          break;
+        }
+      }
+      tok_s[i] = 0x80000000u | (bl << 16) | bd;
+      ++nm;
+      i += bl;
+    }
+    scan[63] = nm;
+  }
+  __syncthreads();
+
+  // -- covered bytes (max-scan of match ends) and the histogram
+  const uint32_t per = (T + blockDim.x - 1) / blockDim.x;
+  const uint32_t i0 = tid * per;
+  uint32_t me = 0;
+  for (uint32_t j = 0; j < per; ++j) {
+    const uint32_t i = i0 + j;
+    const uint32_t tk = i < tl ? tok_s[i] : 0;
+    if (tk) me = max(me, i + ((tk >> 16) & 0x1FFu));
+  }
+  const uint32_t nm = scan[63];
+  __syncthreads();
+  uint32_t run = block_max_excl(me, scan);
+  for (uint32_t j = 0; j < per; ++j) {
+    const uint32_t i = i0 + j;
+    if (i >= tl) break;
+    const uint32_t tk = tok_s[i];
+    if (tk) {
+      const uint32_t len = (tk >> 16) & 0x1FFu;
+      atomicAdd(&hist[257 + len_sym(len)], 1u);
+      atomicAdd(&hist[288 + dist_sym(tk & 0xFFFFu)], 1u);
+      run = max(run, i + len);
+    } else if (run <= i) {
+      atomicAdd(&hist[sd.byte(ts - rs + i)], 1u);
+    }
+  }
+  __syncthreads();
+  uint32_t* gh = reinterpret_cast<uint32_t*>(wk.scratch + t.hist);
+  for (uint32_t i = tid; i < 320; i += blockDim.x) gh[i] = hist[i];
+  uint32_t* gt = reinterpret_cast<uint32_t*>(wk.scratch + t.tok);
+  for (uint32_t i = tid; i < tl; i += blockDim.x) gt[i] = tok_s[i];
+  if (tid == 0) {
+    tp->fin_matches = nm;
+    tp->fix_bits = 0;
+    tp->splice_bit = 0;
+  }
+}
+
+// ---------------------------------------------------------------- Huffman
+// Code lengths for one alphabet, single thread.  Symbols with non-zero
+// frequency are sorted by (frequency, symbol); the two-queue construction
+// (leaves in sorted order, internal nodes in creation order, a leaf wins a
+// tie) builds an optimal tree; if it is deeper than `limit` the per-length
+// counts are adjusted as in ITU-T T.81 Annex K.3 and lengths are handed out
+// longest-first to the least frequent symbols.
+struct HuffScratch {
+  uint16_t sym[288];
+  uint32_t w[288];      // internal node weights
+  uint16_t par[576];    // parent of leaf i (0..m-1) and node k (m+k)
+  uint8_t dep[576];
+  uint32_t cnt[64];
+};
+
+__device__ void huff_lengths(const uint32_t* freq, int n, uint8_t* len, int limit, HuffScratch& s) {
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    len[i] = 0;
+    if (freq[i]) s.sym[m++] = uint16_t(i);
+  }
+  if (m == 0) return;
+  if (m == 1) { len[s.sym[0]] = 1; return; }
+  for (int i = 1; i < m; ++i) {  // insertion sort by (freq, symbol)
+    const uint16_t x = s.sym[i];
+    const uint32_t fx = freq[x];
+    int j = i - 1;
+    while (j >= 0 && freq[s.sym[j]] > fx) { s.sym[j + 1] = s.sym[j]; --j; }
+    s.sym[j + 1] = x;
+  }
+  int li = 0, ni = 0;
+  for (int k = 0; k < m - 1; ++k) {
+    uint32_t wsum = 0;
+    for (int pick = 0; pick < 2; ++pick) {
+      const bool leaf_ok = li < m;
+      const bool node_ok = ni < k;
+      bool take_leaf;
+      if (leaf_ok && node_ok) take_leaf = freq[s.sym[li]] <= s.w[ni];
+      else take_leaf = leaf_ok;
+      if (take_leaf) { wsum += freq[s.sym[li]]; s.par[li] = uint16_t(m + k); ++li; }
+      else { wsum += s.w[ni]; s.par[m + ni] = uint16_t(m + k); ++ni; }
+    }
+    s.w[k] = wsum;
+  }
+  const int root = m + m - 2;
+  s.dep[root] = 0;
+  for (int k = m - 3; k >= 0; --k) s.dep[m + k] = uint8_t(min(63, s.dep[s.par[m + k]] + 1));
+  int maxd = 0;
+  for (int i = 0; i < m; ++i) {
+    s.dep[i] = uint8_t(min(63, s.dep[s.par[i]] + 1));
+    maxd = max(maxd, int(s.dep[i]));
+  }
+  if (maxd <= limit) {
+    for (int i = 0; i < m; ++i) len[s.sym[i]] = s.dep[i];
+    return;
+  }
+  for (int d = 0; d < 64; ++d) s.cnt[d] = 0;
+  for (int i = 0; i < m; ++i) ++s.cnt[s.dep[i]];
+  for (int i = maxd; i > limit; --i) {
+    while (s.cnt[i] > 0) {
+      int j = i - 2;
+      while (s.cnt[j] == 0) --j;
+      s.cnt[i] -= 2;
+      s.cnt[i - 1] += 1;
+      s.cnt[j + 1] += 2;
+      s.cnt[j] -= 1;
+    }
+  }
+  int idx = 0;
+  for (int l = limit; l >= 1; --l)
+    for (uint32_t k = 0; k < s.cnt[l]; ++k) len[s.sym[idx++]] = uint8_t(l);
+}
+
+// Canonical codes (RFC 1951 3.2.2), reversed for LSB-first output.
+__device__ void canon(const uint8_t* len, int n, uint32_t* out /* code | len << 16 */) {
+  uint32_t bl[16] = {0};
+  for (int i = 0; i < n; ++i) bl[len[i]] += len[i] ? 1 : 0;
+  uint32_t next[16];
+  uint32_t code = 0;
+  next[0] = 0;
+  for (int b = 1; b < 16; ++b) { code = (code + bl[b - 1]) << 1; next[b] = code; }
+  for (int i = 0; i < n; ++i) {
+    const uint32_t l = len[i];
+    out[i] = l ? (rev_bits(next[l]++, l) | (l << 16)) : 0u;
+  }
+}
+
+struct BitOut {
+  uint32_t* w;
+  uint32_t pos;
+  __device__ void put(uint32_t v, uint32_t n) {
+    if (!n) return;
+    v &= n == 32 ? kAll : ((1u << n) - 1);
+    const uint32_t i = pos >> 5, sh = pos & 31;
+    w[i] |= v << sh;
+    if (sh + n > 32) w[i + 1] |= v >> (32 - sh);
+    pos += n;
+  }
+};
+
+__constant__ uint8_t c_len_extra[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+__constant__ uint8_t c_dist_extra[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+__constant__ uint8_t c_cl_order[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+
+constexpr int kHuffWarps = 4;
+struct HuffSmem {
+  uint32_t freq[320];
+  uint8_t ll[288], dl[32], cl[19];
+  uint8_t seq[320];
+  uint8_t rsym[320], rext[320];
+  uint32_t clf[19];
+  uint32_t clc[19];
+  HuffScratch hs;
+};
+
+__global__ void __launch_bounds__(kHuffWarps * 32) k_huff(Work wk, const uint32_t* __restrict__ list, uint32_t nlist) {
+  __shared__ HuffSmem S[kHuffWarps];
+  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t si = blockIdx.x * kHuffWarps + wid;
+  if (si >= nlist) return;
+  HuffSmem& H = S[wid];
+  Segment* gp = wk.segs + list[si];
+  const Segment sg = *gp;
+  for (uint32_t b = lane; b < 320; b += 32) {
+    uint32_t f = 0;
+    for (uint32_t t = sg.tile_first; t < sg.tile_first + sg.tile_count; ++t)
+      f += reinterpret_cast<const uint32_t*>(wk.scratch + wk.tiles[t].hist)[b];
+    H.freq[b] = f;
+  }
+  uint32_t mt = 0;
+  for (uint32_t t = sg.tile_first + lane; t < sg.tile_first + sg.tile_count; t += 32) mt += wk.tiles[t].fin_matches;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) mt += __shfl_xor_sync(kAll, mt, o);
+  uint32_t* codes = reinterpret_cast<uint32_t*>(wk.scratch + sg.codes);
+  uint32_t* hdr = reinterpret_cast<uint32_t*>(wk.scratch + sg.hdr_off);
+  for (uint32_t i = lane; i < 256; i += 32) hdr[i] = 0;
+  __syncwarp();
+  if (lane != 0) return;
+
+  H.freq[256] = 1;  // EOB
+  uint32_t type;
+  uint32_t hbits = 0, eob = 0;
+  const uint32_t pieces = sg.len ? (sg.len + 65534) / 65535 : 1;
+  const uint64_t stored_bits = (uint64_t(sg.len) + 5ull * pieces) * 8;
+  if ((sg.flags & kSegWholeBuf) && mt == 0) {
+    type = kBlkStored;  // all-literal parse (block_compressor.cpp:60-61)
+  } else {
+    // fixed cost (deflate_block.cpp:50-70)
+    uint64_t ext = 0;
+    for (int i = 0; i < 29; ++i) ext += uint64_t(c_len_extra[i]) * H.freq[257 + i];
+    for (int i = 0; i < 30; ++i) ext += uint64_t(c_dist_extra[i]) * H.freq[288 + i];
+    uint64_t fixed_bits = 3 + ext;
+    for (int i = 0; i < 288; ++i) fixed_bits += uint64_t(i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : 8) * H.freq[i];
+    for (int i = 0; i < 30; ++i) fixed_bits += 5ull * H.freq[288 + i];
+    // dynamic code (deflate_block.cpp:347-383 conventions)
+    huff_lengths(H.freq, 288, H.ll, 15, H.hs);
+    huff_lengths(H.freq + 288, 32, H.dl, 15, H.hs);
+    if (H.ll[256] == 0) H.ll[256] = 1;
+    bool any = false;
+    for (int i = 0; i < 32; ++i) any |= H.dl[i] != 0;
+    if (!any) H.dl[0] = 1;
+    int hlit = 288, hdist = 32;
+    while (hlit > 257 && H.ll[hlit - 1] == 0) --hlit;
+    while (hdist > 1 && H.dl[hdist - 1] == 0) --hdist;
+    // run-length code of the lengths (deflate_block.cpp:212-242)
+    for (int i = 0; i < hlit; ++i) H.seq[i] = H.ll[i];
+    for (int i = 0; i < hdist; ++i) H.seq[hlit + i] = H.dl[i];
+    const int total = hlit + hdist;
+    int nr = 0;
+    for (int i = 0; i < total;) {
+      const uint8_t v = H.seq[i];
+      int run = 1;
+      while (i + run < total && H.seq[i + run] == v && run < 138) ++run;
+      if (v == 0 && run >= 3) {
+        H.rsym[nr] = run <= 10 ? 17 : 18;
+        H.rext[nr++] = uint8_t(run <= 10 ? run - 3 : run - 11);
+        i += run;
+      } else if (v != 0 && run >= 4) {
+        H.rsym[nr] = v; H.rext[nr++] = 0xFF;
+        ++i;
+        const int rep = min(run - 1, 6);
+        H.rsym[nr] = 16; H.rext[nr++] = uint8_t(rep - 3);
+        i += rep;
+      } else {
+        H.rsym[nr] = v; H.rext[nr++] = 0xFF;
+        ++i;
+      }
+    }
+    for (int i = 0; i < 19; ++i) H.clf[i] = 0;
+    for (int i = 0; i < nr; ++i) ++H.clf[H.rsym[i]];
+    huff_lengths(H.clf, 19, H.cl, 7, H.hs);
+    canon(H.cl, 19, H.clc);
+    int hclen = 19;
+    while (hclen > 4 && H.cl[c_cl_order[hclen - 1]] == 0) --hclen;
+    BitOut bo{hdr, 0};
+    bo.put(uint32_t(hlit - 257), 5);
+    bo.put(uint32_t(hdist - 1), 5);
+    bo.put(uint32_t(hclen - 4), 4);
+    for (int i = 0; i < hclen; ++i) bo.put(H.cl[c_cl_order[i]], 3);
+    for (int i = 0; i < nr; ++i) {
+      const uint32_t c = H.clc[H.rsym[i]];
+      bo.put(c & 0xFFFFu, c >> 16);
+      if (H.rext[i] != 0xFF) bo.put(H.rext[i], H.rsym[i] == 16 ? 2 : H.rsym[i] == 17 ? 3 : 7);
+    }
+    hbits = bo.pos;
+    uint64_t dyn_bits = 3 + hbits + ext;
+    for (int i = 0; i < 288; ++i) dyn_bits += uint64_t(H.ll[i]) * H.freq[i];
+    for (int i = 0; i < 32; ++i) dyn_bits += uint64_t(H.dl[i]) * H.freq[288 + i];
+    if (stored_bits <= fixed_bits && stored_bits <= dyn_bits) type = kBlkStored;
+    else if (fixed_bits <= dyn_bits) type = kBlkFixed;
+    else type = kBlkDynamic;
+  }
+  if (type == kBlkFixed) {
+    for (int i = 0; i < 288; ++i) H.ll[i] = uint8_t(i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : 8);
+    for (int i = 0; i < 32; ++i) H.dl[i] = 5;
+  }
+  if (type != kBlkStored) {
+    canon(H.ll, 288, codes);
+    canon(H.dl, 32, codes + 288);
+    eob = codes[256];
+  }
+  gp->block_type = type;
+  gp->hdr_bits = type == kBlkDynamic ? hbits : 0;
+  gp->eob = eob;
+}
+
+// ---------------------------------------------------------------- k_enc
+__device__ __forceinline__ void ring_put(uint32_t* ring, uint32_t bp, uint32_t v, uint32_t n) {
+  if (!n) return;
+  const uint32_t w = bp >> 5, sh = bp & 31;
+  atomicOr(&ring[w & 127], v << sh);
+  if (sh + n > 32) atomicOr(&ring[(w + 1) & 127], v >> (32 - sh));
+}
+
+constexpr int kEncWarps = 4;
+__global__ void __launch_bounds__(kEncWarps * 32) k_enc(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
+                                                        uint32_t* __restrict__ counter) {
+  __shared__ uint32_t tab[kEncWarps][320];
+  __shared__ uint32_t rings[kEncWarps][128];
+  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* code = tab[wid];
+  uint32_t* ring = rings[wid];
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(counter, 1u);
+    i = __shfl_sync(kAll, i, 0);
+    if (i >= nlist) break;
+    Tile* tp = wk.tiles + list[i];
+    const Tile t = *tp;
+    const Segment sg = wk.segs[t.seg];
+    if (sg.block_type == kBlkStored) {
+      if (lane == 0) { tp->spec_bits = 0; tp->spec_exit = t.start + t.len; }
+      continue;
+    }
+    const uint32_t* gc = reinterpret_cast<const uint32_t*>(wk.scratch + sg.codes);
+    for (uint32_t k = lane; k < 320; k += 32) code[k] = gc[k];
+    for (uint32_t k = lane; k < 128; k += 32) ring[k] = 0;
+    __syncwarp();
+    const uint32_t* tok = reinterpret_cast<const uint32_t*>(wk.scratch + t.tok);
+    uint32_t* out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch);
+    const uint64_t o = sg.in_off;
+    const SegBytes sb{reinterpret_cast<const uint32_t*>(wk.in + (o & ~uint64_t(3))), uint32_t(o & 3)};
+    uint32_t np = 0, cursor = 0, flushed = 0;
+    const uint32_t nwin = (t.len + 31) >> 5;
+    for (uint32_t w = 0; w < nwin; ++w) {
+      const uint32_t wpos = w << 5;
+      const uint32_t lim = min(32u, t.len - wpos);
+      if (np >= wpos + lim) continue;
+      const uint32_t tk = lane < lim ? tok[wpos + lane] : 0u;
+      const uint32_t M = __ballot_sync(kAll, tk != 0);
+      const uint32_t limmask = lim == 32 ? kAll : ((1u << lim) - 1);
+      uint32_t cur = np - wpos, vis = 0;
+      while (cur < lim) {
+        const uint32_t nm = M & limmask & (kAll << cur);
+        if (!nm) { vis |= limmask & (kAll << cur); cur = lim; break; }
+        const uint32_t j = __ffs(nm) - 1;
+        vis |= (kAll << cur) & ((2u << j) - 1u);
+        cur = j + ((__shfl_sync(kAll, tk, j) >> 16) & 0x1FFu);
+      }
+      uint32_t a = 0, na = 0, b = 0, nb = 0;  // two parts of one token
+      if ((vis >> lane) & 1u) {
+        if (tk) {
+          const uint32_t len = (tk >> 16) & 0x1FFu, dist = tk & 0xFFFFu;
+          uint32_t li, le, lv, dc, de, dv;
+          length_code(len, li, le, lv);
+          dist_code(dist, dc, de, dv);
+          const uint32_t lc = code[257 + li], dcw = code[288 + dc];
+          a = (lc & 0xFFFFu) | (lv << (lc >> 16));
+          na = (lc >> 16) + le;
+          b = (dcw & 0xFFFFu) | (dv << (dcw >> 16));
+          nb = (dcw >> 16) + de;
+        } else {
+          const uint32_t c = code[sb.byte(t.start + wpos + lane)];
+          a = c & 0xFFFFu;
+          na = c >> 16;
+        }
+      }
+      uint32_t incl = na + nb;
+#pragma unroll
+      for (int s = 1; s < 32; s <<= 1) {
+        const uint32_t x = __shfl_up_sync(kAll, incl, s);
+        if (lane >= uint32_t(s)) incl += x;
+      }
+      const uint32_t total = __shfl_sync(kAll, incl, 31);
+      const uint32_t bp = cursor + incl - na - nb;
+      ring_put(ring, bp, a, na);
+      ring_put(ring, bp + na, b, nb);
+      cursor += total;
+      np = wpos + cur;
+      __syncwarp();
+      while ((cursor >> 5) >= flushed + 32) {
+        out[flushed + lane] = ring[(flushed + lane) & 127];
+        ring[(flushed + lane) & 127] = 0;
+        flushed += 32;
+        __syncwarp();
+      }
+    }
+    const uint32_t nwords = (cursor + 31) >> 5;
+    for (uint32_t k = flushed + lane; k < nwords; k += 32) out[k] = ring[k & 127];
+    __syncwarp();
+    if (lane == 0) {
+      tp->spec_bits = cursor;
+      tp->spec_exit = t.start + t.len;
+    }
+  }
+}
+
+int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms, Marks* mk) {
+  if (!L.n_tiles) return 0;
+  cudaFuncSetAttribute(k_lz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLz));
+  k_lz<<<L.n_tiles, 1024, kSmemLz, st>>>(wk, L.tiles, L.n_tiles);
+  mk->mark(kPhLazyLz, st);
+  k_huff<<<(L.n_segs + kHuffWarps - 1) / kHuffWarps, kHuffWarps * 32, 0, st>>>(wk, L.segs, L.n_segs);
+  mk->mark(kPhLazyHuff, st);
+  uint32_t blocks = uint32_t(sms) * 8;
+  const uint32_t need = (L.n_tiles + kEncWarps - 1) / kEncWarps;
+  if (blocks > need) blocks = need;
+  k_enc<<<blocks, kEncWarps * 32, 0, st>>>(wk, L.tiles, L.n_tiles, L.counter);
+  mk->mark(kPhLazyEnc, st);
+  return 3;
+}
+
 }  // namespace orotb

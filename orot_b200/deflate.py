@@ -84,6 +84,17 @@ def lib() -> ctypes.CDLL:
     L.deflate_gpu_compress_batch.argtypes = [c.POINTER(c.c_void_p), c.POINTER(c.c_size_t), c.POINTER(c.c_void_p),
                                              c.POINTER(c.c_size_t), c.POINTER(c.c_size_t), c.c_size_t, c.c_int,
                                              c.c_int]
+    L.deflate_gpu_compress_packed.restype = c.c_size_t
+    L.deflate_gpu_compress_packed.argtypes = [c.c_void_p, c.POINTER(c.c_size_t), c.c_size_t, c.c_int, c.c_int,
+                                              c.c_void_p, c.c_size_t, c.POINTER(c.c_uint64), c.POINTER(c.c_size_t)]
+    L.deflate_gpu_packed_bound.restype = c.c_size_t
+    L.deflate_gpu_packed_bound.argtypes = [c.POINTER(c.c_size_t), c.c_size_t, c.c_int]
+    L.deflate_gpu_batch_profile.restype = c.c_int
+    L.deflate_gpu_batch_profile.argtypes = [c.c_void_p, c.c_int]
+    L.deflate_gpu_batch_phase_ms.restype = c.c_int
+    L.deflate_gpu_batch_phase_ms.argtypes = [c.c_void_p, c.POINTER(c.c_float), c.c_int]
+    L.deflate_gpu_phase_name.restype = c.c_char_p
+    L.deflate_gpu_phase_name.argtypes = [c.c_int]
     _lib = L
     return L
 
@@ -172,6 +183,29 @@ def crc32(data, init: int = 0) -> int:
     return r
 
 
+def compress_packed(concat, sizes: Sequence[int], level: int, format: Format, out) -> tuple[int, list, list]:
+    """deflate_gpu_compress_packed: one H2D of `concat`, one D2H into `out`
+    (a writable buffer of at least packed_bound(sizes) bytes).  Returns
+    (packed_total, offsets, sizes)."""
+    L = lib()
+    addr, n, keep = _ptr(concat)
+    oaddr, on, okeep = _ptr(out)
+    cnt = len(sizes)
+    arr = (ctypes.c_size_t * cnt)(*sizes)
+    offs = (ctypes.c_uint64 * (cnt + 1))()
+    szs = (ctypes.c_size_t * cnt)()
+    r = L.deflate_gpu_compress_packed(addr if n else None, arr, cnt, int(level), int(format), oaddr, on, offs, szs)
+    del keep, okeep
+    if r == 0:
+        raise Error(DEFLATE_BUF_ERROR, "compress_packed: " + last_error())
+    return r, list(offs), list(szs)
+
+
+def packed_bound(sizes: Sequence[int], format: Format) -> int:
+    arr = (ctypes.c_size_t * len(sizes))(*sizes)
+    return lib().deflate_gpu_packed_bound(arr, len(sizes), int(format))
+
+
 class DeviceBatch:
     """Buffers kept on the device and compressed by one pass of kernels."""
 
@@ -210,6 +244,16 @@ class DeviceBatch:
 
     def launches(self) -> int:
         return lib().deflate_gpu_batch_launches(self._b)
+
+    def profile(self, on: bool) -> None:
+        lib().deflate_gpu_batch_profile(self._b, int(on))
+
+    def phase_ms(self) -> dict:
+        arr = (ctypes.c_float * 16)()
+        n = lib().deflate_gpu_batch_phase_ms(self._b, arr, 16)
+        if n < 0:
+            raise Error(DEFLATE_PARAM_ERROR, "phase_ms: " + last_error())
+        return {lib().deflate_gpu_phase_name(i).decode(): float(arr[i]) for i in range(n)}
 
     def close(self) -> None:
         if self._b:

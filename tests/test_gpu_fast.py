@@ -77,16 +77,40 @@ def test_multi_tile_whole_buffer_matches_oracle(gpu, oracle, kind, level):
         assert inflate(out, 2) == d
 
 
+def parallel_c(gpu, data, level, fmt, block, cap):
+    """deflate_parallel_compress through the C ABI with an explicit capacity."""
+    import ctypes
+    L = gpu.lib()
+    ctx = L.deflate_parallel_new(level, fmt, 8, block)
+    out = ctypes.create_string_buffer(cap)
+    r = L.deflate_parallel_compress(ctx, data, len(data), out, cap)
+    L.deflate_parallel_free(ctx)
+    return out.raw[:r]
+
+
 @pytest.mark.parametrize("block", [0, 1000, 32768, 65537, 262144])
 def test_parallel_fast_matches_oracle(gpu, oracle, block):
     for kind in (0, 2, 4, 5):
         d = synth.gen(900001, kind, block + kind)
         for level in (0, 1, 3):
             for fmt in (0, 1, 2):
-                out = gpu.ParallelCompressor(level, gpu.Format(fmt), 8, block).compress(d)
+                out = parallel_c(gpu, d, level, fmt, block, 2 * len(d) + 1024)
                 ref = oracle.parallel(d, level, fmt, block)
                 assert out == ref, (kind, level, fmt, block)
     assert inflate(out, 2) == d
+
+
+def test_parallel_overflow_returns_zero(gpu, oracle):
+    """Stored chunks of 1000 bytes cost 5 bytes each, so the pigz stream is
+    larger than deflate_compress_bound(); the reference writes past such a
+    buffer (src/parallel/parallel_compressor.cpp:108-120 never checks), the
+    engine returns 0 instead."""
+    import ctypes
+    d = synth.gen(900001, 3, 1)
+    L = gpu.lib()
+    bound = L.deflate_compress_bound(len(d), 2)
+    assert len(oracle.parallel(d, 0, 2, 1000)) > bound
+    assert parallel_c(gpu, d, 0, 2, 1000, bound) == b""
 
 
 def test_empty_and_tiny_inputs(gpu, oracle):
