@@ -151,6 +151,25 @@ size_t deflate_gpu_compress_packed(const void* in_concat, const size_t* in_sizes
                                    size_t* out_sizes);
 size_t deflate_gpu_packed_bound(const size_t* in_sizes, size_t count, deflate_format format);
 
+/* No-allocation variant (no counterpart in the reference).  For callers that
+ * own every byte of device memory and cannot let a library call cudaMalloc
+ * (a host framework's pool allocator, a fixed device-memory budget): inputs,
+ * output and the output size are the caller's device pointers, and the only
+ * working memory is a static device array of about 2.4 MB that every GPU
+ * loading this library keeps until exit.  deflate_compress semantics for
+ * levels 0-3 (same bytes); inputs up to DEFLATE_GPU_NOALLOC_MAX_INPUT bytes;
+ * out_capacity must be at least deflate_compress_bound().  Asynchronous on
+ * cuda_stream (NULL = legacy default stream); *d_out_size receives the
+ * compressed size.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race and must be ordered by the caller.
+ * Returns 0 when the work was enqueued; -1 bad pointer or format, -2 input
+ * too large, -3 level above 3, -4 capacity below the bound, -5 device
+ * set-up failed, -6 launch failed (orot_b200_last_error() says which). */
+#define DEFLATE_GPU_NOALLOC_MAX_INPUT (1u << 20)
+int deflate_gpu_compress_noalloc(const void* d_in, size_t in_size, void* d_out, size_t out_capacity, int level,
+                                 deflate_format format, unsigned long long* d_out_size, void* cuda_stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* orot_b200_last_error(void);
 

@@ -469,3 +469,242 @@ void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t
 }
 
 }  // namespace orotb
+
+// ====================================================================== no-allocation entry point
+// Some callers cannot let a library allocate device memory: code that runs
+// inside another framework's memory pool or under a fixed device-memory
+// budget, where every byte on the GPU is owned by the caller.  They can still
+// use the fast levels through deflate_gpu_compress_noalloc(): the caller
+// passes device pointers for the input, the output and the output size, and
+// the only working memory is the file-scope array below, which every GPU
+// that loads this library holds until the process exits.  It keeps a padded
+// copy of the input (so no read ever runs past the caller's buffer) and the
+// token bit stream.  The kernel writes every word of it that it later reads,
+// so nothing has to start at zero, but all calls share it: two calls whose
+// kernels overlap on the GPU (different streams, or different host threads)
+// race on it and must be ordered by the caller.
+#include <mutex>
+#include <string>
+#include "../../include/orot_b200.h"
+
+namespace orotb {
+
+void set_error(const std::string& e);  // engine.cu
+
+constexpr uint32_t kNoAllocInBytes = DEFLATE_GPU_NOALLOC_MAX_INPUT + 256;
+constexpr uint32_t kNoAllocBitBytes = DEFLATE_GPU_NOALLOC_MAX_INPUT / 8 * 9 + 256;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[(kNoAllocInBytes + kNoAllocBitBytes) / 4];
+
+template <int HB>
+__global__ void __launch_bounds__(256) k_noalloc(const uint8_t* __restrict__ in, uint32_t n, uint8_t* __restrict__ out,
+                                                  int level_arg, int lv, int fmt, uint32_t* scratch,
+                                                  unsigned long long* out_size) {
+  extern __shared__ uint32_t sm[];
+  constexpr int H = 1 << HB;
+  uint32_t* head = sm;
+  uint32_t* ring = head + H;
+  uint32_t* wbuf = ring + kRing;
+  __shared__ uint32_t crc_tab[256];
+  __shared__ uint32_t part_crc[224], part_a[224], part_b[224], part_len[224];
+  __shared__ uint32_t x2k[64];
+  __shared__ uint32_t s_bits, s_matches;
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  uint8_t* cin = reinterpret_cast<uint8_t*>(scratch);
+  uint32_t* bits = scratch + kNoAllocInBytes / 4;
+
+  // padded copy of the input; the tail is zeroed so over-reads see zeros
+  for (uint32_t i = tid; i < n + 256; i += blockDim.x) cin[i] = i < n ? in[i] : 0;
+  for (uint32_t i = tid; i < 256; i += blockDim.x) {
+    uint32_t c = i;
+    for (int k = 0; k < 8; ++k) c = (c & 1) ? (c >> 1) ^ kCrcPoly : (c >> 1);
+    crc_tab[i] = c;
+  }
+  if (tid == 0) {
+    uint32_t x = 0x40000000u;
+    for (int k = 0; k < 64; ++k) { x2k[k] = x; x = gf2_mulmod(x, x); }
+    s_bits = 0;
+    s_matches = 0;
+  }
+  __syncthreads();
+
+  if (wid == 0) {
+    if (lv >= 1) {
+      const TileView tv{SegBytes{reinterpret_cast<const uint32_t*>(cin), 0}, n, 0, n};
+      const WinState r = walk_tile<HB>(tv, nullptr, head, ring, wbuf, bits, nullptr, nullptr);
+      if (lane == 0) { s_bits = r.cursor; s_matches = r.matches; }
+    }
+  } else {
+    // checksum partials over 224 contiguous parts
+    const uint32_t t = tid - 32, per = (n + 223) / 224;
+    const uint32_t b0 = min(n, t * per), b1 = min(n, b0 + per);
+    uint32_t crc = 0, A = 0, B = 0;
+    for (uint32_t i = b0; i < b1; ++i) {
+      const uint32_t by = cin[i];
+      crc = crc_tab[(crc ^ by) & 0xFF] ^ (crc >> 8);
+      A += by;
+      if (A >= 65521u) A -= 65521u;
+      B += A;
+      if (B >= 65521u) B -= 65521u;
+    }
+    part_crc[t] = crc;
+    part_a[t] = A;
+    part_b[t] = B;
+    part_len[t] = b1 - b0;
+  }
+  __syncthreads();
+
+  __shared__ uint32_t s_type, s_check;
+  __shared__ unsigned long long s_total;
+  if (tid == 0) {
+    CrcPowers pw;
+    for (int k = 0; k < 64; ++k) pw.x2k[k] = x2k[k];
+    uint32_t crc = 0;
+    uint64_t s1 = 1, s2 = 0;
+    for (int t = 0; t < 224; ++t) {
+      if (!part_len[t]) continue;
+      crc = gf2_mulmod(xpow8n(pw, part_len[t]), crc) ^ part_crc[t];
+      s2 = (s2 + uint64_t(part_len[t] % 65521u) * s1 + part_b[t]) % 65521u;
+      s1 = (s1 + part_a[t]) % 65521u;
+    }
+    s_check = fmt == kFmtGzip ? ~(gf2_mulmod(xpow8n(pw, n), 0xFFFFFFFFu) ^ crc) : uint32_t(s2 << 16) | uint32_t(s1);
+    // block type: level 0 and all-literal parses are stored
+    // (src/compress/block_compressor.cpp:53-63, src/deflate/deflate_block.cpp:414-421)
+    uint32_t type = kBlkStored;
+    if (lv >= 1 && s_matches) {
+      const uint64_t fixed_bits = 3ull + s_bits + 7;
+      const uint64_t stored_bits = (uint64_t(n) + 5) * 8;
+      type = stored_bits <= fixed_bits ? kBlkStored : kBlkFixed;
+    }
+    s_type = type;
+    const uint64_t hdr = fmt == kFmtZlib ? 2 : fmt == kFmtGzip ? 10 : 0;
+    const uint64_t trl = fmt == kFmtZlib ? 4 : fmt == kFmtGzip ? 8 : 0;
+    const uint64_t pieces = n ? (n + 65534) / 65535 : 1;
+    const uint64_t raw = type == kBlkStored ? uint64_t(n) + 5 * pieces : (3ull + s_bits + 7 + 7) / 8;
+    s_total = hdr + raw + trl;
+  }
+  __syncthreads();
+  const uint32_t hdr = fmt == kFmtZlib ? 2 : fmt == kFmtGzip ? 10 : 0;
+  const uint64_t total = s_total;
+  const uint32_t trl = fmt == kFmtZlib ? 4 : fmt == kFmtGzip ? 8 : 0;
+  uint8_t* raw = out + hdr;
+  const uint64_t raw_len = total - hdr - trl;
+  if (s_type == kBlkFixed) {
+    // 3 header bits (BFINAL=1, BTYPE=01), the token bits, 7 zero bits of EOB
+    const uint32_t nb = s_bits;
+    for (uint64_t k = tid; k < raw_len; k += blockDim.x) {
+      uint32_t v = 0;
+      const int64_t s = int64_t(k) * 8 - 3;  // token bit of output bit 0 of this byte
+      for (int j = 0; j < 8; ++j) {
+        const int64_t b = s + j;
+        uint32_t bit;
+        if (b < 0) bit = (3u >> (j)) & 1u;       // the 3 header bits: value 0b011
+        else if (uint64_t(b) < nb) bit = (bits[b >> 5] >> (b & 31)) & 1u;
+        else bit = 0;                            // EOB and padding
+        v |= bit << j;
+      }
+      raw[k] = uint8_t(v);
+    }
+  } else {
+    // stored pieces of at most 65535 bytes (deflate_block.cpp:107-132)
+    for (uint64_t k = tid; k < raw_len; k += blockDim.x) {
+      const uint64_t piece = k / 65540, off = k % 65540;
+      const uint64_t start = piece * 65535;
+      const uint32_t len = uint32_t(min(uint64_t(65535), uint64_t(n) - min(uint64_t(n), start)));
+      uint8_t v;
+      if (off == 0) v = (start + len == n) ? 1 : 0;
+      else if (off == 1) v = uint8_t(len);
+      else if (off == 2) v = uint8_t(len >> 8);
+      else if (off == 3) v = uint8_t(~len);
+      else if (off == 4) v = uint8_t(~len >> 8);
+      else v = cin[start + off - 5];
+      raw[k] = v;
+    }
+  }
+  if (tid == 0) {
+    if (fmt == kFmtZlib) {
+      out[0] = 0x78; out[1] = 0x9C;
+      for (int i = 0; i < 4; ++i) out[total - 4 + i] = uint8_t(s_check >> (24 - 8 * i));
+    } else if (fmt == kFmtGzip) {
+      const uint8_t xfl = level_arg >= 9 ? 2 : (level_arg <= 2 ? 4 : 0);
+      const uint8_t h[10] = {0x1F, 0x8B, 8, 0, 0, 0, 0, 0, xfl, 0xFF};
+      for (int i = 0; i < 10; ++i) out[i] = h[i];
+      for (int i = 0; i < 4; ++i) {
+        out[total - 8 + i] = uint8_t(s_check >> (8 * i));
+        out[total - 4 + i] = uint8_t(n >> (8 * i));
+      }
+    }
+    *out_size = total;
+  }
+}
+
+// Device address of g_noalloc_scratch, looked up once per device (with that
+// device current) on the first call made on it.
+static uint32_t* noalloc_scratch_ptr(int dev) {
+  static std::mutex mu;
+  static uint32_t* ptrs[64] = {};
+  static bool init[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!init[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+      return nullptr;
+    }
+    ptrs[dev] = static_cast<uint32_t*>(p);
+    init[dev] = true;
+  }
+  return ptrs[dev];
+}
+
+}  // namespace orotb
+
+extern "C" int deflate_gpu_compress_noalloc(const void* d_in, size_t in_size, void* d_out, size_t out_capacity,
+                                            int level, deflate_format format, unsigned long long* d_out_size,
+                                            void* cuda_stream) {
+  using namespace orotb;
+  const int fmt = int(format);
+  if ((in_size && !d_in) || !d_out || !d_out_size || fmt < 0 || fmt > 2) {
+    set_error("deflate_gpu_compress_noalloc: null pointer or unknown format");
+    return -1;
+  }
+  if (in_size > DEFLATE_GPU_NOALLOC_MAX_INPUT) {
+    set_error("deflate_gpu_compress_noalloc: input larger than DEFLATE_GPU_NOALLOC_MAX_INPUT (1 MiB)");
+    return -2;
+  }
+  const int lv = level < 0 ? 0 : level > 12 ? 12 : level;
+  if (lv > 3) {
+    set_error("deflate_gpu_compress_noalloc: only levels 0-3 are available without allocation");
+    return -3;
+  }
+  const size_t bound = in_size + (in_size >> 12) + (in_size >> 14) + (in_size >> 25) + 13 +
+                       (fmt == kFmtZlib ? 6 : fmt == kFmtGzip ? 18 : 0);
+  if (out_capacity < bound) {
+    set_error("deflate_gpu_compress_noalloc: out_capacity below deflate_compress_bound()");
+    return -4;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); set_error("no CUDA device"); return -5; }
+  uint32_t* scratch = noalloc_scratch_ptr(dev);
+  if (!scratch) return -5;
+  cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+  const uint8_t* in = static_cast<const uint8_t*>(d_in);
+  uint8_t* out = static_cast<uint8_t*>(d_out);
+  const uint32_t n = uint32_t(in_size);
+  if (lv == 1 || lv == 0) {
+    const size_t smem = (size_t(1 << 12) + kRing + kWbuf) * 4;
+    k_noalloc<12><<<1, 256, smem, st>>>(in, n, out, level, lv, fmt, scratch, d_out_size);
+  } else {
+    const size_t smem = (size_t(1 << 14) + kRing + kWbuf) * 4;
+    cudaFuncSetAttribute(k_noalloc<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    k_noalloc<14><<<1, 256, smem, st>>>(in, n, out, level, lv, fmt, scratch, d_out_size);
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("deflate_gpu_compress_noalloc launch: ") + cudaGetErrorString(e));
+    return -6;
+  }
+  return 0;
+}
