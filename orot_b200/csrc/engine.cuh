@@ -69,7 +69,8 @@ struct WinRec {
   uint32_t entry;      // first parse position >= window start (tile-relative)
   uint32_t bit;        // bit offset of that token in the tile's stream
   uint32_t matches;    // match tokens before it
-  uint32_t pad;
+  uint32_t run;        // D when all 32 positions have candidate distance D <= 32
+                       // and equal the bytes D earlier (a run window), else 0
 };
 
 struct Tile {

@@ -37,6 +37,9 @@ constexpr uint32_t kFull = 0xFFFFFFFFu;
 __device__ __forceinline__ uint32_t hash_fast(uint32_t v, int hb) { return (v * 0x9E3779B1u) >> (32 - hb); }
 
 // ---------------------------------------------------------------- k_lastocc
+// Each thread hashes 16 consecutive positions from 6 loaded words; a position
+// followed by one with the same hash (runs) needs no atomic, since the later
+// position wins the max anyway.
 template <int HB>
 __global__ void __launch_bounds__(256) k_lastocc(Work wk, const uint32_t* __restrict__ list, uint32_t nlist) {
   extern __shared__ uint32_t tbl[];
@@ -47,14 +50,30 @@ __global__ void __launch_bounds__(256) k_lastocc(Work wk, const uint32_t* __rest
   for (int i = threadIdx.x; i < H; i += blockDim.x) tbl[i] = 0;
   __syncthreads();
   const uint64_t a = sg.in_off;
-  const SegBytes sb{reinterpret_cast<const uint32_t*>(wk.in + (a & ~uint64_t(3))), uint32_t(a & 3)};
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(wk.in + (a & ~uint64_t(3)));
+  const uint32_t boff = uint32_t(a & 3);
   const uint32_t end = t.start + t.len;
-  for (uint32_t base = t.start + (threadIdx.x & ~31u); base < end; base += blockDim.x) {
-    const uint32_t p = base + (threadIdx.x & 31);
-    const bool ins = p < end && p + 4 <= sg.len;
-    const uint32_t h = ins ? hash_fast(sb.load4(p), HB) : kFull;
-    const uint32_t peers = __match_any_sync(kFull, h);
-    if (ins && (peers >> (threadIdx.x & 31)) == 1u) atomicMax(&tbl[h], p);
+  const uint32_t lim = sg.len >= 4 ? min(end, sg.len - 3) : t.start;  // positions with 4 bytes
+  for (uint32_t base = t.start + 16 * threadIdx.x; base < lim; base += 16 * blockDim.x) {
+    const uint32_t q = base + boff;
+    const uint32_t* qw = w + (q >> 2);
+    const uint32_t sh = q & 3;
+    uint32_t W[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) W[j] = __ldg(qw + j);
+    uint32_t h[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const uint32_t k = sh + i;
+      h[i] = hash_fast(__funnelshift_r(W[k >> 2], W[(k >> 2) + 1], (k & 3) * 8), HB);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const uint32_t p = base + i;
+      if (p >= lim) break;
+      if (i < 15 && p + 1 < lim && h[i] == h[i + 1]) continue;
+      atomicMax(&tbl[h[i]], p);
+    }
   }
   __syncthreads();
   uint32_t* slot = reinterpret_cast<uint32_t*>(wk.scratch + t.slot);
@@ -83,53 +102,90 @@ __global__ void __launch_bounds__(256) k_carry_scan(Work wk, const uint32_t* __r
 
 // ---------------------------------------------------------------- the walker
 // Per-warp shared state: head[] (walk only), the bit ring, and the staged
-// bytes of the current window (16 words starting at the word that holds the
-// window's first byte: positions wpos .. wpos+35 and the next window's
-// prefix).
-constexpr uint32_t kRing = 128, kWbuf = 16;
+// bytes around the current window: 24 words starting 32 bytes before the
+// window (so runs with a period up to 32 can be checked) and reaching 64
+// bytes past its start (the p side of every capped match length).
+constexpr uint32_t kRing = 128, kWbuf = 24;
+constexpr uint32_t kCapMax = 48;  // capped match length of lane 0 (48 - lane)
 
 struct WinState {
   uint32_t np, cursor, flushed, matches, tokens;
 };
 
-// Stages 16 words of segment bytes starting at position wpos (rounded down to
-// a word) into wbuf; returns the byte offset of wpos inside wbuf.
+// Staging starts at segment position max(wpos - 32, 0), rounded down to a
+// word.  Returns the byte offset of wpos inside wbuf.
+__device__ __forceinline__ uint32_t stage_base_word(const SegBytes& sb, uint32_t wpos) {
+  return (sb.boff + (wpos >= 32 ? wpos - 32 : 0)) >> 2;
+}
+__device__ __forceinline__ uint32_t prefetch_window(const SegBytes& sb, uint32_t wpos, uint32_t lane) {
+  return lane < kWbuf ? __ldg(sb.w + stage_base_word(sb, wpos) + lane) : 0u;
+}
 __device__ __forceinline__ uint32_t stage_window(const SegBytes& sb, uint32_t wpos, uint32_t* wbuf, uint32_t lane,
                                                  uint32_t pre) {
   if (lane < kWbuf) wbuf[lane] = pre;
   __syncwarp();
-  return (wpos + sb.boff) & 3;
-}
-__device__ __forceinline__ uint32_t prefetch_window(const SegBytes& sb, uint32_t wpos, uint32_t lane) {
-  return lane < kWbuf ? __ldg(sb.w + ((wpos + sb.boff) >> 2) + lane) : 0u;
+  return sb.boff + wpos - 4 * stage_base_word(sb, wpos);
 }
 __device__ __forceinline__ uint32_t wload4(const uint32_t* wbuf, uint32_t off) {
   return __funnelshift_r(wbuf[off >> 2], wbuf[(off >> 2) + 1], (off & 3) * 8);
 }
 
 // Capped common-prefix length of the bytes at p (staged at wbuf offset po)
-// and at q (global), at most cap <= 32.  The q-side words are loaded in one
-// batch so the lane pays one memory latency.
+// and at q (global), at most cap <= kCapMax.  The first 8 q-side words are
+// loaded in one batch (one memory latency covers matches up to ~24 bytes);
+// longer matches fetch one more word per step.  The loop runs while any lane
+// of the warp is still matching, so its trip count follows the longest match
+// in the window rather than the cap.  Every lane of the warp must call it.
 __device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_t* wbuf, uint32_t po, uint32_t q,
-                                               uint32_t cap) {
+                                               uint32_t cap, bool active) {
+  constexpr int PRE = 8;
   const uint32_t qa = q + sb.boff;
   const uint32_t* qw = sb.w + (qa >> 2);
   const uint32_t qs = (qa & 3) * 8;
-  const uint32_t nw = (cap + 3 + (qa & 3)) / 4 + 1;  // words needed, <= 10
-  uint32_t v[10];
+  uint32_t v[PRE];
 #pragma unroll
-  for (int j = 0; j < 10; ++j) v[j] = (uint32_t(j) < nw) ? __ldg(qw + j) : 0u;
+  for (int j = 0; j < PRE; ++j) v[j] = active && uint32_t(j) * 4 < cap + 4 ? __ldg(qw + j) : 0u;
   uint32_t n = 0;
-  bool open = true;
+  bool open = active && cap > 0;
 #pragma unroll
-  for (int j = 0; j < 9; ++j) {
-    if (open && n < cap) {
+  for (int j = 0; j < PRE - 1; ++j) {
+    if (!__any_sync(kFull, open)) break;
+    if (open) {
       const uint32_t x = wload4(wbuf, po + 4 * j) ^ __funnelshift_r(v[j], v[j + 1], qs);
       if (x) { n += (__ffs(x) - 1) >> 3; open = false; } else { n += 4; }
+      if (n >= cap) open = false;
+    }
+  }
+  uint32_t lo = v[PRE - 1];
+  for (uint32_t j = PRE - 1; __any_sync(kFull, open); ++j) {
+    if (open) {
+      const uint32_t hi = __ldg(qw + j + 1);
+      const uint32_t x = wload4(wbuf, po + 4 * j) ^ __funnelshift_r(lo, hi, qs);
+      lo = hi;
+      if (x) { n += (__ffs(x) - 1) >> 3; open = false; } else { n += 4; }
+      if (n >= cap) open = false;
     }
   }
   return n < cap ? n : cap;
 }
+
+// head[] entry: the candidate's position mod 32768 with a valid bit (u16)
+// beside its first byte (u8).  That is all the reference's fast path uses of
+// a candidate (distance = (p - cand) & 0x7FFF, first-byte check at cand), and
+// keeping the byte saves a dependent load.  Position 0 stays invalid (head
+// value 0 means empty in src/deflate/lz77.cpp:178).
+struct HeadTab {
+  uint16_t* pos;   // (pos & 0x7FFF) | 0x8000 when valid, 0 when empty
+  uint8_t* byte;
+  __device__ __forceinline__ void put(uint32_t h, uint32_t p, uint32_t b) const {
+    pos[h] = p ? uint16_t((p & 0x7FFFu) | 0x8000u) : uint16_t(0);
+    byte[h] = uint8_t(b);
+  }
+};
+// Shared-memory words per warp of a walker: head table (2 + 1 bytes per
+// entry), bit ring and staged window.
+template <int HB>
+__host__ __device__ constexpr uint32_t walker_words() { return ((1u << HB) * 3 + 3) / 4 + kRing + kWbuf; }
 
 // Greedy parse and fixed-Huffman emission of one 32-position window.  Lane
 // `lane` holds position wpos+lane; `d` is its candidate distance (0 = none).
@@ -139,12 +195,17 @@ __device__ __forceinline__ void parse_window(const SegBytes& sb, uint32_t n, uin
   const uint32_t p = wpos + lane;
   uint32_t clen = 0;
   bool exact = true;
-  if (d && p >= st.np && lane < lim) {
-    const uint32_t maxm = min(258u, n - p);
-    const uint32_t cap = min(maxm, max(3u, 32u - lane));
-    clen = lcp_window(sb, wbuf, woff + lane, p - d, cap);
-    exact = clen < cap || cap == maxm;
-    if (clen < 3) clen = 0;
+  const bool want = d && p >= st.np && lane < lim;
+  const uint32_t maxm = want ? min(258u, n - p) : 0u;
+  const uint32_t cap = want ? min(maxm, max(3u, kCapMax - lane)) : 0u;
+  if (__any_sync(kFull, want)) {
+    clen = lcp_window(sb, wbuf, woff + lane, want ? p - d : p, cap, want);
+    if (want) {
+      exact = clen < cap || cap == maxm;
+      if (clen < 3) clen = 0;
+    } else {
+      clen = 0;
+    }
   }
   const uint32_t M = __ballot_sync(kFull, clen >= 3);
   const uint32_t limmask = lim == 32 ? kFull : ((1u << lim) - 1);
@@ -233,17 +294,23 @@ __device__ __forceinline__ TileView tile_view(const Work& wk, const Tile& t, con
 
 // Speculative walk of one tile (parse entry = tile start): inserts every
 // position into head[], records the candidate distance of every position and
-// the parse entry of every window, emits the fixed-Huffman bits.
+// the parse entry (and run period) of every window, emits the fixed-Huffman
+// bits.  `carry` holds full segment positions (0 = empty).
 template <int HB>
-__device__ WinState walk_tile(const TileView& tv, const uint32_t* carry, uint32_t* head, uint32_t* ring,
+__device__ WinState walk_tile(const TileView& tv, const uint32_t* carry, uint32_t* smem_warp, uint32_t* ring,
                               uint32_t* wbuf, uint32_t* out, WinRec* rec, uint16_t* cand16) {
   constexpr int H = 1 << HB;
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t lt = (1u << lane) - 1;
+  const HeadTab head{reinterpret_cast<uint16_t*>(smem_warp), reinterpret_cast<uint8_t*>(smem_warp) + 2 * H};
   if (carry) {
-    for (int i = lane; i < H; i += 32) head[i] = __ldg(carry + i);
+#pragma unroll 8
+    for (int i = lane; i < H; i += 32) {
+      const uint32_t pos = __ldg(carry + i);
+      head.put(i, pos, pos ? tv.sb.byte(pos) : 0u);
+    }
   } else {
-    for (int i = lane; i < H; i += 32) head[i] = 0;
+    for (int i = lane; i < H; i += 32) head.put(i, 0, 0);
   }
   for (uint32_t i = lane; i < kRing; i += 32) ring[i] = 0;
   __syncwarp();
@@ -255,24 +322,44 @@ __device__ WinState walk_tile(const TileView& tv, const uint32_t* carry, uint32_
     const uint32_t wpos = tv.ts + (w << 5);
     const uint32_t woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
     if (w + 1 < nwin) pre = prefetch_window(tv.sb, wpos + 32, lane);
-    if (rec && lane == 0) rec[w] = WinRec{st.np - tv.ts, st.cursor, st.matches, st.tokens};
+    const WinRec rc{st.np - tv.ts, st.cursor, st.matches, 0};
     const uint32_t p = wpos + lane;
     const bool ins = p < tend && p + 4 <= tv.n;
     const uint32_t v4 = wload4(wbuf, woff + lane);
     const uint32_t h = ins ? hash_fast(v4, HB) : kFull;
     const uint32_t peers = __match_any_sync(kFull, h);
     const uint32_t before = peers & lt;
-    uint32_t cand = 0;
-    if (ins) cand = before ? (wpos + 31 - __clz(before)) : head[h];
+    const uint32_t src = before ? 31 - __clz(before) : lane;
+    const uint32_t vb = __shfl_sync(kFull, v4, src);
+    uint32_t cpos = 0, cbyte = 0;  // candidate: position mod 32768 | valid bit, first byte
+    if (ins) {
+      if (before) {
+        const uint32_t c = wpos + src;
+        cpos = c ? ((c & 0x7FFFu) | 0x8000u) : 0u;
+        cbyte = vb & 0xFFu;
+      } else {
+        cpos = head.pos[h];
+        cbyte = head.byte[h];
+      }
+    }
     __syncwarp();
-    if (ins && (peers >> lane) == 1u) head[h] = p;
+    if (ins && (peers >> lane) == 1u) head.put(h, p, v4 & 0xFFu);
     // candidate distance after the first-byte check at the candidate itself
     uint32_t d = 0;
-    if (ins && cand != 0) {
-      const uint32_t dist = (p - cand) & 0x7FFFu;
-      if (dist != 0 && tv.sb.byte(cand) == (v4 & 0xFFu)) d = dist;
+    if (cpos & 0x8000u) {
+      const uint32_t dist = (p - (cpos & 0x7FFFu)) & 0x7FFFu;
+      if (dist != 0 && cbyte == (v4 & 0xFFu)) d = dist;
     }
     if (cand16 && p < tend) cand16[p - tv.ts] = uint16_t(d);
+    if (rec) {
+      // run window: every position has the same short distance D and its
+      // four bytes equal the four bytes D earlier
+      const uint32_t D = __shfl_sync(kFull, d, 0);
+      const bool ok = wpos >= 32 && D != 0 && D <= 32 && d == D && p + 4 <= tend &&
+                      wload4(wbuf, woff + lane - D) == v4;
+      const uint32_t all = __ballot_sync(kFull, ok);
+      if (lane == 0) rec[w] = WinRec{rc.entry, rc.bit, rc.matches, all == kFull ? D : 0u};
+    }
     __syncwarp();
     const uint32_t lim = min(32u, tend - wpos);
     if (st.np < wpos + lim) parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st);
@@ -282,7 +369,9 @@ __device__ WinState walk_tile(const TileView& tv, const uint32_t* carry, uint32_
 }
 
 // Re-parse of one tile from `entry` using the recorded candidate distances,
-// until the parse meets the speculative one at a window boundary.
+// until the parse meets the speculative one at a window boundary.  Inside
+// runs of short period (see WinRec::run) every match is (258, D), so the
+// re-parse steps through them arithmetically.
 struct FixOut {
   uint32_t bits, matches, exit, merged, merge_win;
 };
@@ -297,9 +386,47 @@ __device__ FixOut fix_tile(const TileView& tv, uint32_t entry, const WinRec* rec
   const uint32_t nwin = (tv.tl + 31) >> 5;
   for (uint32_t w = (entry - tv.ts) >> 5; w < nwin; ++w) {
     const uint32_t wpos = tv.ts + (w << 5);
-    if (st.np == tv.ts + rec[w].entry) { r.merged = 1; r.merge_win = w; break; }
+    const WinRec rc = rec[w];
+    if (st.np == tv.ts + rc.entry) { r.merged = 1; r.merge_win = w; break; }
     const uint32_t lim = min(32u, tend - wpos);
     if (st.np >= wpos + lim) continue;
+    if (rc.run) {
+      // extent of the run: windows w.. with the same period
+      const uint32_t D = rc.run;
+      uint32_t wend = nwin;
+      for (uint32_t b = w + 1; b < nwin; b += 32) {
+        const bool stop = b + lane < nwin && rec[b + lane].run != D;
+        const uint32_t m = __ballot_sync(kFull, stop);
+        if (m) { wend = b + __ffs(m) - 1; break; }
+      }
+      const uint32_t rend = tv.ts + (wend << 5);  // bytes before rend all repeat at distance D
+      if (st.np + 258 <= rend) {
+        const uint32_t k = (rend - st.np) / 258;
+        uint32_t code, nb;
+        fixed_match(258, D, code, nb);
+        for (uint32_t t0 = 0; t0 < k; t0 += 32) {
+          const uint32_t cnt = min(32u, k - t0);
+          if (lane < cnt) {
+            const uint32_t bp = st.cursor + lane * nb, wd = bp >> 5, sh = bp & 31;
+            atomicOr(&ring[wd & (kRing - 1)], code << sh);
+            if (sh + nb > 32) atomicOr(&ring[(wd + 1) & (kRing - 1)], code >> (32 - sh));
+          }
+          st.cursor += cnt * nb;
+          __syncwarp();
+          while ((st.cursor >> 5) >= st.flushed + 32) {
+            out[st.flushed + lane] = ring[(st.flushed + lane) & (kRing - 1)];
+            ring[(st.flushed + lane) & (kRing - 1)] = 0;
+            st.flushed += 32;
+            __syncwarp();
+          }
+        }
+        st.np += 258 * k;
+        st.matches += k;
+        st.tokens += k;
+        w = ((st.np - tv.ts) >> 5) - 1;  // continue at the window holding np
+        continue;
+      }
+    }
     const uint32_t pre = prefetch_window(tv.sb, wpos, lane);
     const uint32_t woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
     const uint32_t d = lane < lim ? cand16[(w << 5) + lane] : 0u;
@@ -317,10 +444,10 @@ template <int HB, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_walk(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
                                                       uint32_t* __restrict__ counter) {
   extern __shared__ uint32_t sm[];
-  constexpr int H = 1 << HB;
+  constexpr uint32_t HW = ((1u << HB) * 3 + 3) / 4;
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* head = sm + wid * (H + kRing + kWbuf);
-  uint32_t* ring = head + H;
+  uint32_t* head = sm + wid * walker_words<HB>();
+  uint32_t* ring = head + HW;
   uint32_t* wbuf = ring + kRing;
   for (;;) {
     uint32_t i = 0;
@@ -440,7 +567,7 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
     k_carry_scan<HB><<<g, 256, 0, st>>>(wk, L.multi, L.n_multi);
   }
   mk->mark(kPhPre, st);
-  const size_t wsm = size_t(WARPS) * (H + kRing + kWbuf) * 4;
+  const size_t wsm = size_t(WARPS) * walker_words<HB>() * 4;
   if (L.n_walk) {
     cudaFuncSetAttribute(k_walk<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm));
     int per_sm = 0;
@@ -500,9 +627,9 @@ __global__ void __launch_bounds__(256) k_noalloc(const uint8_t* __restrict__ in,
                                                   int level_arg, int lv, int fmt, uint32_t* scratch,
                                                   unsigned long long* out_size) {
   extern __shared__ uint32_t sm[];
-  constexpr int H = 1 << HB;
+  constexpr uint32_t HW = ((1u << HB) * 3 + 3) / 4;
   uint32_t* head = sm;
-  uint32_t* ring = head + H;
+  uint32_t* ring = head + HW;
   uint32_t* wbuf = ring + kRing;
   __shared__ uint32_t crc_tab[256];
   __shared__ uint32_t part_crc[224], part_a[224], part_b[224], part_len[224];
@@ -694,10 +821,10 @@ extern "C" int deflate_gpu_compress_noalloc(const void* d_in, size_t in_size, vo
   uint8_t* out = static_cast<uint8_t*>(d_out);
   const uint32_t n = uint32_t(in_size);
   if (lv == 1 || lv == 0) {
-    const size_t smem = (size_t(1 << 12) + kRing + kWbuf) * 4;
+    const size_t smem = size_t(walker_words<12>()) * 4;
     k_noalloc<12><<<1, 256, smem, st>>>(in, n, out, level, lv, fmt, scratch, d_out_size);
   } else {
-    const size_t smem = (size_t(1 << 14) + kRing + kWbuf) * 4;
+    const size_t smem = size_t(walker_words<14>()) * 4;
     cudaFuncSetAttribute(k_noalloc<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     k_noalloc<14><<<1, 256, smem, st>>>(in, n, out, level, lv, fmt, scratch, d_out_size);
   }
