@@ -151,6 +151,40 @@ size_t deflate_gpu_compress_packed(const void* in_concat, const size_t* in_sizes
                                    size_t* out_sizes);
 size_t deflate_gpu_packed_bound(const size_t* in_sizes, size_t count, deflate_format format);
 
+/* Pipelined host-to-host batch (no counterpart in the reference): as
+ * deflate_gpu_compress_packed, but the buffers are split into groups of about
+ * group_bytes (0 = 512 MiB) and `lanes` passes (0 = 3) are kept in flight, so
+ * the copies of one group overlap the kernels of another.  Group g's outputs
+ * start at the sum of the packed bounds of groups before it; out_offsets[i]
+ * are absolute, out_offsets[count] is the end of the last output.  Returns
+ * that end, or 0 on error. */
+size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_sizes, size_t count, int level,
+                                      deflate_format format, void* out_packed, size_t out_capacity,
+                                      uint64_t* out_offsets, size_t* out_sizes, size_t group_bytes, int lanes);
+
+/* Continuous-batching server (no counterpart in the reference).  A server
+ * thread keeps up to `lanes` passes (0 = 3) on the GPU; whenever one
+ * finishes, every pending request that fits the device-memory budget
+ * (0 = 16 GiB) is admitted into the next pass, so requests that arrive while
+ * others run join the next pass and passes overlap on the device.  Each
+ * request has deflate_compress semantics at its own level and format, so its
+ * bytes do not depend on its batch.
+ *   submit: `in` and `out` must stay valid until wait returns; returns a
+ *           ticket (0 on error).  An `out_capacity` below
+ *           deflate_compress_bound() is accepted and makes that request fail
+ *           alone if its output does not fit.
+ *   wait:   0 done (*out_size, *latency_s = submit to completion), -2 failed,
+ *           1 timed out (ticket still valid), -1 unknown ticket.
+ *   stats:  passes issued and the most passes seen in flight at once. */
+typedef struct deflate_gpu_server deflate_gpu_server;
+deflate_gpu_server* deflate_gpu_server_new(size_t device_budget, int lanes);
+void deflate_gpu_server_free(deflate_gpu_server* s);
+uint64_t deflate_gpu_server_submit(deflate_gpu_server* s, const void* in, size_t in_size, void* out, size_t out_capacity,
+                                   int level, deflate_format format);
+int deflate_gpu_server_wait(deflate_gpu_server* s, uint64_t ticket, size_t* out_size, double* latency_s,
+                            double timeout_s);
+int deflate_gpu_server_stats(deflate_gpu_server* s, uint64_t* passes, uint64_t* max_in_flight);
+
 /* No-allocation variant (no counterpart in the reference).  For callers that
  * own every byte of device memory and cannot let a library call cudaMalloc
  * (a host framework's pool allocator, a fixed device-memory budget): inputs,

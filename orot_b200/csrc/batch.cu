@@ -40,6 +40,20 @@ __global__ void k_pack_offsets(const Stream* __restrict__ st, uint32_t n, uint64
 }
 
 __global__ void k_pack(const Stream* __restrict__ st, uint32_t n, const uint64_t* __restrict__ off,
+                       const uint8_t* __restrict__ out, uint8_t* __restrict__ packed);
+
+__global__ void k_sizes(const Stream* __restrict__ st, uint32_t n, uint64_t* __restrict__ sizes) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) sizes[i] = st[i].error ? 0 : st[i].out_size;
+}
+
+void launch_pack(const Work& w, uint64_t* d_off, uint64_t* d_sizes, uint8_t* d_packed, cudaStream_t st) {
+  k_pack_offsets<<<1, 1024, 0, st>>>(w.streams, w.nstreams, d_off);
+  k_pack<<<w.nstreams, 256, 0, st>>>(w.streams, w.nstreams, d_off, w.out, d_packed);
+  if (d_sizes) k_sizes<<<(w.nstreams + 255) / 256, 256, 0, st>>>(w.streams, w.nstreams, d_sizes);
+}
+
+__global__ void k_pack(const Stream* __restrict__ st, uint32_t n, const uint64_t* __restrict__ off,
                        const uint8_t* __restrict__ out, uint8_t* __restrict__ packed) {
   const uint32_t i = blockIdx.x;
   if (i >= n) return;

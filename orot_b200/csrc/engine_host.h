@@ -91,4 +91,9 @@ class Engine {
 std::mutex& global_mutex();
 Engine& global_engine();
 
+// Packs every stream's output of the last pass at 16-byte aligned offsets
+// (d_off: count + 1 entries, the last the total) and optionally writes the
+// sizes (0 = failed stream).  Defined in batch.cu.
+void launch_pack(const Work& w, uint64_t* d_off, uint64_t* d_sizes, uint8_t* d_packed, cudaStream_t st);
+
 }  // namespace orotb

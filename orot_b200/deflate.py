@@ -95,6 +95,21 @@ def lib() -> ctypes.CDLL:
     L.deflate_gpu_batch_phase_ms.argtypes = [c.c_void_p, c.POINTER(c.c_float), c.c_int]
     L.deflate_gpu_phase_name.restype = c.c_char_p
     L.deflate_gpu_phase_name.argtypes = [c.c_int]
+    L.deflate_gpu_compress_pipelined.restype = c.c_size_t
+    L.deflate_gpu_compress_pipelined.argtypes = [c.c_void_p, c.POINTER(c.c_size_t), c.c_size_t, c.c_int, c.c_int,
+                                                 c.c_void_p, c.c_size_t, c.POINTER(c.c_uint64),
+                                                 c.POINTER(c.c_size_t), c.c_size_t, c.c_int]
+    L.deflate_gpu_server_new.restype = c.c_void_p
+    L.deflate_gpu_server_new.argtypes = [c.c_size_t, c.c_int]
+    L.deflate_gpu_server_free.argtypes = [c.c_void_p]
+    L.deflate_gpu_server_submit.restype = c.c_uint64
+    L.deflate_gpu_server_submit.argtypes = [c.c_void_p, c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.c_int,
+                                            c.c_int]
+    L.deflate_gpu_server_wait.restype = c.c_int
+    L.deflate_gpu_server_wait.argtypes = [c.c_void_p, c.c_uint64, c.POINTER(c.c_size_t), c.POINTER(c.c_double),
+                                          c.c_double]
+    L.deflate_gpu_server_stats.restype = c.c_int
+    L.deflate_gpu_server_stats.argtypes = [c.c_void_p, c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     _lib = L
     return L
 
@@ -199,6 +214,83 @@ def compress_packed(concat, sizes: Sequence[int], level: int, format: Format, ou
     if r == 0:
         raise Error(DEFLATE_BUF_ERROR, "compress_packed: " + last_error())
     return r, list(offs), list(szs)
+
+
+def compress_pipelined(concat, sizes: Sequence[int], level: int, format: Format, out, group_bytes: int = 0,
+                       lanes: int = 0) -> tuple[int, list, list]:
+    """deflate_gpu_compress_pipelined; `out` needs packed_bound(sizes) bytes."""
+    L = lib()
+    addr, n, keep = _ptr(concat)
+    oaddr, on, okeep = _ptr(out)
+    cnt = len(sizes)
+    arr = (ctypes.c_size_t * cnt)(*sizes)
+    offs = (ctypes.c_uint64 * (cnt + 1))()
+    szs = (ctypes.c_size_t * cnt)()
+    r = L.deflate_gpu_compress_pipelined(addr if n else None, arr, cnt, int(level), int(format), oaddr, on, offs, szs,
+                                         int(group_bytes), int(lanes))
+    del keep, okeep
+    if r == 0:
+        raise Error(DEFLATE_BUF_ERROR, "compress_pipelined: " + last_error())
+    return r, list(offs), list(szs)
+
+
+class Server:
+    """Continuous-batching compression server (deflate_gpu_server_*).
+
+    submit() returns a ticket; the input and output buffers must stay alive
+    until wait() returns for that ticket."""
+
+    def __init__(self, device_budget: int = 0, lanes: int = 0):
+        self._s = lib().deflate_gpu_server_new(int(device_budget), int(lanes))
+        if not self._s:
+            raise Error(DEFLATE_MEM_ERROR, "server: " + last_error())
+        self._keep = {}
+
+    def submit(self, data, level: int, format: Format, out=None, out_capacity: int | None = None) -> int:
+        addr, n, keep = _ptr(data)
+        if out is None:
+            cap = compress_bound(n, format) if out_capacity is None else out_capacity
+            out = ctypes.create_string_buffer(max(cap, 1))
+        else:
+            cap = len(out) if out_capacity is None else out_capacity
+        oaddr, _, okeep = _ptr(out)
+        t = lib().deflate_gpu_server_submit(self._s, addr if n else None, n, oaddr, cap, int(level), int(format))
+        if t == 0:
+            raise Error(DEFLATE_PARAM_ERROR, "server submit: " + last_error())
+        self._keep[t] = (keep, okeep, out)
+        return t
+
+    def wait(self, ticket: int, timeout: float = 0.0):
+        """(bytes or None on failure, latency seconds); raises TimeoutError."""
+        sz = ctypes.c_size_t(0)
+        lat = ctypes.c_double(0)
+        r = lib().deflate_gpu_server_wait(self._s, ticket, ctypes.byref(sz), ctypes.byref(lat), float(timeout))
+        if r == 1:
+            raise TimeoutError(f"ticket {ticket}")
+        keep = self._keep.pop(ticket, None)
+        if r == -1:
+            raise Error(DEFLATE_PARAM_ERROR, f"unknown ticket {ticket}")
+        if r != 0:
+            return None, lat.value
+        out = keep[2]
+        buf = bytes(memoryview(out).cast("B")[:sz.value])
+        return buf, lat.value
+
+    def stats(self) -> tuple[int, int]:
+        a, b = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        lib().deflate_gpu_server_stats(self._s, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def close(self) -> None:
+        if self._s:
+            lib().deflate_gpu_server_free(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
 
 
 def packed_bound(sizes: Sequence[int], format: Format) -> int:

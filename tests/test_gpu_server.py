@@ -1,0 +1,105 @@
+"""GPU tests of the continuous-batching server and the pipelined batch.
+
+The server admits requests that arrive while other passes run into the next
+pass; each request is its own stream, so its bytes must be identical alone
+(deflate_compress) and in any mix, and a request whose output does not fit
+must fail alone without disturbing the requests batched with it."""
+import random
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from orot_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(count, seed, max_size=2 << 20):
+    rng = random.Random(seed)
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(1), np.log(max_size))))
+        kind = rng.randint(0, 5)
+        level = rng.choice([0, 1, 1, 1, 2, 3, 6, 6, 9])
+        fmt = rng.randint(0, 2)
+        out.append((synth.gen(n, kind, seed * 1000 + i), level, fmt))
+    return out
+
+
+def test_server_alone_equals_mix(gpu):
+    reqs = _requests(80, 1)
+    singles = [gpu.compress(d, lv, gpu.Format(f)) for d, lv, f in reqs]
+    srv = gpu.Server(device_budget=4 << 30, lanes=3)
+    tickets = [srv.submit(d, lv, gpu.Format(f)) for d, lv, f in reqs]
+    for t, ref in zip(tickets, singles):
+        out, lat = srv.wait(t, timeout=120)
+        assert out == ref
+        assert lat >= 0
+    passes, _ = srv.stats()
+    assert passes >= 1
+    srv.close()
+
+
+def test_server_poisoned_request_fails_alone(gpu):
+    reqs = _requests(12, 2, max_size=1 << 20)
+    srv = gpu.Server(lanes=2)
+    tickets = []
+    for i, (d, lv, f) in enumerate(reqs):
+        cap = 8 if i == 5 else None  # far too small: this request must fail alone
+        tickets.append(srv.submit(d, lv, gpu.Format(f), out_capacity=cap))
+    for i, (t, (d, lv, f)) in enumerate(zip(tickets, reqs)):
+        out, _ = srv.wait(t, timeout=120)
+        if i == 5 and len(d) > 0:
+            assert out is None
+        else:
+            assert out == gpu.compress(d, lv, gpu.Format(f))
+    srv.close()
+
+
+def test_server_arrivals_overlap_passes(gpu):
+    """Requests submitted from another thread while passes run: several
+    passes end up in flight together and every result stays exact."""
+    reqs = _requests(150, 3, max_size=4 << 20)
+    srv = gpu.Server(device_budget=1 << 30, lanes=3)
+    tickets = [None] * len(reqs)
+
+    def producer():
+        for i, (d, lv, f) in enumerate(reqs):
+            tickets[i] = srv.submit(d, lv, gpu.Format(f))
+            time.sleep(0.0005)
+
+    th = threading.Thread(target=producer)
+    th.start()
+    th.join()
+    for t, (d, lv, f) in zip(tickets, reqs):
+        out, _ = srv.wait(t, timeout=300)
+        assert out == gpu.compress(d, lv, gpu.Format(f))
+    passes, inflight = srv.stats()
+    assert passes >= 2
+    assert inflight >= 2
+    srv.close()
+
+
+def test_server_small_budget_still_completes(gpu):
+    reqs = [(synth.gen(8 << 20, k, k), 1, 1) for k in range(4)]
+    srv = gpu.Server(device_budget=96 << 20, lanes=2)
+    ts = [srv.submit(d, lv, gpu.Format(f)) for d, lv, f in reqs]
+    for t, (d, lv, f) in zip(ts, reqs):
+        out, _ = srv.wait(t, timeout=120)
+        assert out == gpu.compress(d, lv, gpu.Format(f))
+    srv.close()
+
+
+def test_pipelined_batch_equals_single_calls(gpu):
+    sizes = [int(x) for x in synth.loguniform_sizes(200, 1024, 2 << 20, 7)]
+    bufs = [synth.array(n, i % 4, i + 3) for i, n in enumerate(sizes)]
+    concat = np.concatenate(bufs)
+    out = np.zeros(gpu.packed_bound(sizes, gpu.Format.Zlib), np.uint8)
+    end, offs, szs = gpu.compress_pipelined(concat, sizes, 1, gpu.Format.Zlib, out, group_bytes=16 << 20, lanes=3)
+    assert end == offs[-1]
+    for i, b in enumerate(bufs):
+        ref = gpu.compress(b, 1, gpu.Format.Zlib)
+        assert szs[i] == len(ref)
+        assert out[offs[i]:offs[i] + szs[i]].tobytes() == ref
