@@ -2,7 +2,7 @@
 """Headline benchmark: batched DEFLATE compression on one (or N) B200s.
 
 Workload: 10,000 independent zlib streams, buffer sizes drawn log-uniformly
-from 1 KiB to 4 MiB (seed 11, about 4 GiB), buffer i filled by generator
+from 1 KiB to 4 MiB (seed 11, 5.13 GB), buffer i filled by generator
 i mod 4 (Zipf text, sorted u32 deltas, zeros, random bytes; see
 orot_b200/synth.py), level 1, deflate_compress semantics per buffer (one
 block per buffer, byte-identical to the reference).  All buffers are
@@ -11,15 +11,19 @@ compressed by one pass of kernels replayed from a CUDA graph.
 Reported (one JSON line from rank 0):
   value      GB/s (decimal, input bytes / device time) with the inputs already
              in HBM, CUDA events on the launching stream, max over ranks;
-  e2e        the same through deflate_gpu_compress_packed from pinned host
-             memory: host->device copy, kernels, packing and the
-             device->host copy of every compressed stream inside the timing;
+  e2e        the same through deflate_gpu_compress_pipelined from pinned host
+             memory: host->device copies, kernels, packing and the
+             device->host copies of every compressed stream inside the timing
+             (groups of buffers in flight so copies overlap kernels);
   plain      one pass per buffer on a sample (device-resident and through
              deflate_compress), the comparison the batch is measured against;
   roofline   the dominant kernel phase against the measured HBM copy peak;
   cpu_baseline  the reference's own deflate_compress (oracle/_ref) on the
-             host cores over a bounded sample.
-Inputs (4 GiB) exceed the 126 MB L2, so no flush is needed between steps.
+             host cores over a bounded sample;
+  serving    Poisson arrivals (2,000 requests/s, 4 KiB-16 MiB, 70% level 1 /
+             30% level 6, raw) through the continuous-batching server: p50/p99
+             latency and sustained GB/s, beside the plain path.
+Inputs (5.1 GB) exceed the 126 MB L2, so no flush is needed between steps.
 
 `--impl reference` times the reference's CPU implementation on the same
 workload (bounded samples per step) and prints the same line.
@@ -62,6 +66,8 @@ def parse():
     ap.add_argument("--level", type=int, default=1)
     ap.add_argument("--plain-sample", type=int, default=300)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
     return ap.parse_args()
 
 
@@ -229,6 +235,71 @@ def run_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------- serving
+def measure_serving(deflate, buf, total, count, rate, seed=0):
+    """Open-loop Poisson arrivals at `rate` requests/s: sizes log-uniform in
+    4 KiB-16 MiB, 70% level 1 / 30% level 6, raw DEFLATE, payloads cut from
+    the mixed workload buffer.  Latency is submission to completion measured
+    by the server; sustained GB/s is the bytes over first submission to last
+    completion.  The same requests, one deflate_compress call at a time, give
+    the plain comparison (on a prefix of the trace)."""
+    from orot_b200 import synth
+    rng = np.random.default_rng(13 + seed)
+    sizes = [int(x) for x in synth.loguniform_sizes(count, 4096, 16 << 20, 13 + seed)]
+    levels = [1 if u < 0.7 else 6 for u in rng.random(count)]
+    starts = [int(rng.integers(0, max(1, total - n))) for n in sizes]
+    gaps = rng.exponential(1.0 / rate, count)
+    caps = [deflate.compress_bound(n, deflate.Format.Raw) for n in sizes]
+    outs = np.empty(sum(caps), np.uint8)
+    ooff = np.concatenate([[0], np.cumsum(caps)])
+    srv = deflate.Server(device_budget=16 << 30, lanes=3)
+    tickets = [0] * count
+    t0 = time.perf_counter()
+    due = t0
+    for i in range(count):
+        due += gaps[i]
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        tickets[i] = srv.submit(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw,
+                                out=outs[ooff[i]:ooff[i + 1]])
+    lat = []
+    for i in range(count):
+        o, l = srv.wait(tickets[i], timeout=600)
+        if o is None:
+            raise SystemExit(f"served request {i} failed")
+        lat.append(l)
+    t_end = time.perf_counter()
+    passes, inflight = srv.stats()
+    # spot-check exactness against single calls
+    for i in range(0, count, max(1, count // 25)):
+        ref = deflate.compress(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw)
+        o = outs[ooff[i]:ooff[i] + len(ref)].tobytes()
+        if o != ref:
+            raise SystemExit(f"served request {i} differs from deflate_compress")
+    srv.close()
+    nbytes = sum(sizes)
+    # plain path: the same requests, one deflate_compress at a time
+    k = min(count, 200)
+    pl = []
+    tp = time.perf_counter()
+    for i in range(k):
+        a = time.perf_counter()
+        deflate.compress(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw)
+        pl.append(time.perf_counter() - a)
+    tp = time.perf_counter() - tp
+    lat_ms = np.array(lat) * 1e3
+    return {"requests": count, "rate_req_s": rate, "offered_GBps": nbytes / gaps.sum() / 1e9,
+            "sustained_GBps": nbytes / (t_end - t0) / 1e9,
+            "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+            "passes": passes, "max_passes_in_flight": inflight, "levels": "70% L1 / 30% L6", "format": "raw",
+            "sizes": "log-uniform 4 KiB-16 MiB", "budget_GiB": 16,
+            "plain": {"requests": k, "GBps": sum(sizes[:k]) / tp / 1e9,
+                      "p50_ms": float(np.percentile(np.array(pl) * 1e3, 50)),
+                      "p99_ms": float(np.percentile(np.array(pl) * 1e3, 99)),
+                      "note": "one deflate_compress per request, back to back (service time, no queueing)"}}
+
+
 # ---------------------------------------------------------------- GPU arm
 def main():
     args = parse()
@@ -357,20 +428,26 @@ def main():
     if not args.no_e2e:
         obound = deflate.packed_bound(sizes, deflate.Format.Zlib)
         outp = torch.empty(obound, dtype=torch.uint8, pin_memory=True).numpy()
-        deflate.compress_packed(buf[:total], sizes, args.level, deflate.Format.Zlib, outp)  # warm-up
+        deflate.compress_pipelined(buf[:total], sizes, args.level, deflate.Format.Zlib, outp)  # warm-up
         barrier()
         t0 = time.perf_counter()
         steps_e2e = max(1, min(args.steps, 3))
         packed = 0
         for _ in range(steps_e2e):
-            packed, poffs, psz = deflate.compress_packed(buf[:total], sizes, args.level, deflate.Format.Zlib, outp)
+            packed, poffs, psz = deflate.compress_pipelined(buf[:total], sizes, args.level, deflate.Format.Zlib, outp)
         dt = (time.perf_counter() - t0) / steps_e2e
         barrier()
         dt = max_over_ranks(dt)
         if psz != out_sizes:
             raise SystemExit("end-to-end sizes differ from the device-resident pass")
         e2e = {"value": world * total / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": total,
-               "d2h_bytes_per_step": int(packed) + 8 * (len(sizes) + 1), "ms_per_step": dt * 1e3}
+               "d2h_bytes_per_step": int(comp) + 16 * (len(sizes) + 1), "ms_per_step": dt * 1e3,
+               "api": "deflate_gpu_compress_pipelined (pinned host buffers, 512 MiB groups, 3 passes in flight)"}
+
+    # -- serving: Poisson arrivals through the continuous-batching server
+    serving = None
+    if args.serve_requests > 0:
+        serving = measure_serving(deflate, buf, total, args.serve_requests, args.serve_rate, seed=rank)
 
     # -- CPU baseline: the reference on the host cores (rank 0, N = 1 only)
     cpu = None
@@ -391,7 +468,7 @@ def main():
                        "format": "zlib", "graph": True, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}"},
             "ratio": ratio, "gpu_launches": launches_per_pass * args.steps, "e2e": e2e, "plain": plain,
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -77,6 +77,11 @@ Engine::Engine() {
     const long t = std::strtol(v, nullptr, 10);
     if (t >= 32 && t <= 65536 && t % 32 == 0) tile_override = uint32_t(t);
   }
+  // Lazy-level run length override (tiles per CTA, 1..kLazyRun) for tests.
+  if (const char* v = std::getenv("OROT_B200_LAZY_RUN")) {
+    const long r = std::strtol(v, nullptr, 10);
+    if (r >= 1 && r <= long(kLazyRun)) lazy_run_override = uint32_t(r);
+  }
 }
 Engine::~Engine() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -171,7 +176,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
           tiles.push_back(tl);
         }
       } else if (lv >= 4) {
-        // independent 8 KiB tiles, each with its own token words and histogram
+        // independent 4 KiB tiles, each with its own token words and histogram
         const uint32_t LT = kLazyTile;
         const uint32_t nt = len ? uint32_t((len + LT - 1) / LT) : 1;
         g.tile_count = nt;
@@ -225,6 +230,21 @@ bool Engine::plan(const std::vector<Job>& jobs) {
   off_segs = put_table(buf, segs);
   off_tiles = put_table(buf, tiles);
   off_ck = put_table(buf, cks);
+  // Lazy tiles go to CTAs in runs of consecutive tiles of one segment (the
+  // window slides from tile to tile); runs shorten when there are too few
+  // tiles to give every SM several.
+  if (!lists[kLazySegs].empty()) {
+    const uint32_t n = uint32_t(lists[kLazyTiles].size());
+    const uint32_t R = lazy_run_override ? lazy_run_override
+                                         : std::max(1u, std::min(kLazyRun, n / (4u * uint32_t(sms))));
+    for (uint32_t si : lists[kLazySegs]) {
+      const Segment& g = segs[si];
+      for (uint32_t t = 0; t < g.tile_count; t += R) {
+        lists[kLazyRuns].push_back(g.tile_first + t);
+        lists[kLazyRuns].push_back(std::min(R, g.tile_count - t));
+      }
+    }
+  }
   for (int i = 0; i < kNumLists; ++i) off_lists[i] = put_table(buf, lists[i]);
   off_counters = align_up(buf.size(), 256);
   buf.resize(off_counters + 256, 0);
@@ -287,6 +307,8 @@ bool Engine::launch(cudaStream_t st) {
   }
   if (!lists[kLazyTiles].empty()) {
     LazyLists L{};
+    L.runs = list(kLazyRuns);
+    L.n_runs = uint32_t(lists[kLazyRuns].size() / 2);
     L.tiles = list(kLazyTiles);
     L.n_tiles = uint32_t(lists[kLazyTiles].size());
     L.segs = list(kLazySegs);

@@ -131,11 +131,13 @@ __host__ __device__ inline uint64_t tile_stream_bytes(uint32_t tile_len) { retur
 // bits and a match at most 48 bits per 3 covered bytes (16 bits per byte).
 __host__ __device__ inline uint64_t lazy_stream_bytes(uint32_t tile_len) { return align_up(uint64_t(tile_len) * 2 + 256, 128); }
 
-// Levels 4+: tiles of 32 x 258 bytes, each searching a 32 KiB window before
+// Levels 4+: tiles of 16 x 258 bytes, each searching a 32 KiB window before
 // it.  A multiple of the longest match keeps runs of 258-byte matches (zero
 // fill, short periods) aligned with tile boundaries, so cutting the input
-// into independent tiles costs no extra token on such data.
-constexpr uint32_t kLazyTile = 32 * 258;
+// into independent tiles costs no extra token on such data.  One CTA walks a
+// run of kLazyRun consecutive tiles, sliding its window.
+constexpr uint32_t kLazyTile = 16 * 258;
+constexpr uint32_t kLazyRun = 16;
 constexpr uint32_t kLazyWindow = 32768;
 
 }  // namespace orotb

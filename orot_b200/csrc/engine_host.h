@@ -46,7 +46,7 @@ struct Job {
 enum ListId {
   kLast12, kMulti12, kWalk12,
   kLast14, kMulti14, kWalk14,
-  kLazyTiles, kLazySegs,
+  kLazyTiles, kLazySegs, kLazyRuns,
   kNumLists
 };
 
@@ -71,6 +71,7 @@ class Engine {
   HostBuf h_tables, h_stage;
   cudaGraphExec_t graph_exec = nullptr;
   uint32_t tile_override = 0;
+  uint32_t lazy_run_override = 0;
 
   // planned tables (host copies)
   std::vector<Stream> streams;

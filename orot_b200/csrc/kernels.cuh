@@ -34,7 +34,9 @@ struct FastLists {
 
 // Index lists for the lazy-level (4-12) pipeline.
 struct LazyLists {
-  const uint32_t* tiles;     // tiles to match + parse
+  const uint32_t* runs;      // (first tile, tile count) of every run, count <= kLazyRun
+  uint32_t n_runs;
+  const uint32_t* tiles;     // tiles to encode
   uint32_t n_tiles;
   const uint32_t* segs;      // segments needing Huffman tables
   uint32_t n_segs;

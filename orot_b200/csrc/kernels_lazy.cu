@@ -40,16 +40,19 @@ namespace {
 
 constexpr uint32_t kAll = 0xFFFFFFFFu;
 constexpr uint32_t T = kLazyTile, W = kLazyWindow;
-constexpr uint32_t kRegion = W + T;                 // positions with links
-constexpr uint32_t kDataBytes = 41472;             // >= W + T + 16 (align) + 16 (tail)
+constexpr uint32_t kRegion = W + T;                            // positions with links
+constexpr uint32_t kDataBytes = (W + T + 48 + 127) / 128 * 128;  // + align + over-read tail
 constexpr uint32_t kLinkBytes = (kRegion * 2 + 127) / 128 * 128;  // u16 per position
-constexpr uint32_t kTblBytes = T * 8 > 65536 ? T * 8 : 65536;      // u16 x 2^15 table, later F[T] + G[T]
+constexpr uint32_t kTblBytes = 65536;                          // u16 per 15-bit hash, kept across a run
+constexpr uint32_t kDupBytes = 1u << 15;                       // u8 per 15-bit hash (link construction)
+constexpr uint32_t kFgBytes = T * 8 > kDupBytes ? T * 8 : kDupBytes;  // F[T] + G[T], aliasing dup
+constexpr uint32_t kTokBytes = T * 4;
 constexpr uint32_t kFmWords = T / 32;
+constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFgBytes + kTokBytes + kFmWords * 4 + 320 * 4 +
+                             64 * 4;
 static_assert(T % 32 == 0, "tiles are whole windows of 32 positions");
-constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFmWords * 4 + 320 * 4 + 64 * 4;
-static_assert(kDataBytes >= W + T + 32, "data area");
-static_assert(T * 8 <= kTblBytes, "F and G fit the table area");
-static_assert(T * 4 <= kLinkBytes, "token words fit the link area");
+static_assert(kSmemLz <= 227 * 1024, "one CTA per SM");
+static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words of links");
 
 struct LazyCfg { int chain, nice, lazy, miss; };
 __constant__ LazyCfg c_lazy[13] = {
@@ -95,6 +98,9 @@ __device__ uint32_t lz_search(const SmemBytes& sd, const uint16_t* __restrict__ 
       continue;
     }
     misses = 0;
+    // a candidate that differs at byte best cannot beat best (the reference's
+    // quick reject, src/deflate/lz77.cpp:137-142); it changes no result
+    if (best >= 4 && best < maxm && sd.byte(q + best) != sd.byte(r + best)) continue;
     uint32_t len = 4;
     while (len < maxm) {
       const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
@@ -105,7 +111,7 @@ __device__ uint32_t lz_search(const SmemBytes& sd, const uint16_t* __restrict__ 
     if (len > best) {
       best = len;
       bd = r - q;
-      if (int(len) >= nice) break;
+      if (int(len) >= nice || len >= maxm) break;  // nothing can beat maxm
     }
   }
   return best >= 3 ? (best << 16) | bd : 0u;
@@ -150,151 +156,210 @@ __device__ __forceinline__ uint32_t dist_sym(uint32_t d) {
 }  // namespace
 
 // ---------------------------------------------------------------- k_lz
-__global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restrict__ list, uint32_t nlist) {
+// One CTA per run of up to kLazyRun consecutive tiles of a segment.  The
+// links of the window and the hash table carry from one tile to the next
+// (shifted down by the tile length), so each position is linked once.
+__global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restrict__ runs, uint32_t nruns) {
   extern __shared__ __align__(16) uint8_t sm[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(sm);
   uint16_t* link = reinterpret_cast<uint16_t*>(sm + kDataBytes);
   uint16_t* tbl = reinterpret_cast<uint16_t*>(sm + kDataBytes + kLinkBytes);
-  uint32_t* F = reinterpret_cast<uint32_t*>(sm + kDataBytes + kLinkBytes);
+  uint8_t* fgb = sm + kDataBytes + kLinkBytes + kTblBytes;
+  uint32_t* F = reinterpret_cast<uint32_t*>(fgb);
   uint32_t* G = F + T;
-  uint32_t* fm = reinterpret_cast<uint32_t*>(sm + kDataBytes + kLinkBytes + kTblBytes);
+  uint8_t* dup = fgb;  // only while linking
+  uint32_t* tok_s = reinterpret_cast<uint32_t*>(fgb + kFgBytes);
+  uint32_t* fm = tok_s + T;
   uint32_t* hist = fm + kFmWords;
   uint32_t* scan = hist + 320;
-  uint32_t* tok_s = reinterpret_cast<uint32_t*>(link);  // after the searches
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
-  if (blockIdx.x >= nlist) return;
-  Tile* tp = wk.tiles + list[blockIdx.x];
-  const Tile t = *tp;
-  const Segment sg = wk.segs[t.seg];
+  if (blockIdx.x >= nruns) return;
+  const uint32_t first = runs[2 * blockIdx.x];
+  const uint32_t last = first + runs[2 * blockIdx.x + 1];
+  const Segment sg = wk.segs[wk.tiles[first].seg];
   const LazyCfg cfg = c_lazy[sg.level];
-  const uint32_t ts = t.start, tl = t.len, tend = ts + tl;
-  const uint32_t rs = ts > W ? ts - W : 0;           // region start (segment-relative)
-  const uint32_t nreg = tend - rs;                    // positions with links
-  const uint32_t copy_end = min(sg.len, tend + 8);    // bytes staged
-  // -- stage bytes [rs, copy_end) at 16-byte granularity
-  const uint64_t g0 = (sg.in_off + rs) & ~uint64_t(15);
-  const uint32_t boff = uint32_t(sg.in_off + rs - g0);
-  const uint32_t n16 = (boff + (copy_end - rs) + 15) / 16;
-  const uint4* src = reinterpret_cast<const uint4*>(wk.in + g0);
-  uint4* dst = reinterpret_cast<uint4*>(sm);
-  for (uint32_t i = tid; i < kDataBytes / 16; i += blockDim.x)
-    dst[i] = i < n16 ? __ldg(src + i) : make_uint4(0, 0, 0, 0);
-  for (uint32_t i = tid; i < kTblBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(tbl)[i] = kAll;
-  for (uint32_t i = tid; i < 320; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  const SmemBytes sd{sdata, boff};
-
-  // -- links: previous position with the same 15-bit hash (warp 0, in order)
-  if (wid == 0) {
-    const uint32_t lt = (1u << lane) - 1;
-    for (uint32_t base = 0; base < nreg; base += 32) {
-      const uint32_t x = base + lane;
-      const bool valid = x < nreg && rs + x + 4 <= sg.len;
-      const uint32_t h = valid ? hash15(sd.load4(x)) : kAll;
-      const uint32_t peers = __match_any_sync(kAll, h);
-      const uint32_t before = peers & lt;
-      uint32_t l = 0;
-      if (valid) {
-        const uint32_t pred = before ? base + 31 - __clz(before) : tbl[h];
-        l = pred == 0xFFFFu ? 0u : x - pred;
-      }
-      if (x < nreg) link[x] = uint16_t(l);
-      __syncwarp();
-      if (valid && (peers >> lane) == 1u) tbl[h] = uint16_t(x);
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-
-  // -- searches at every tile position (whole warps per iteration: T is a
-  // multiple of 32)
   const uint32_t lazy_chain = cfg.chain > 1 ? uint32_t(cfg.chain) >> 1 : 1u;
-  for (uint32_t i = tid; i < T; i += blockDim.x) {
-    uint32_t f = 0, g = 0;
-    if (i < tl && i + 4 <= tl) {
-      const uint32_t r = ts - rs + i;
-      const uint32_t v = sd.load4(r);
-      const uint32_t maxm = min(258u, tl - i);
-      f = lz_search(sd, link, r, kAll, maxm, cfg.chain, cfg.nice, cfg.miss, v);
-      if (cfg.lazy) g = lz_search(sd, link, r, r - 1, maxm, int(lazy_chain), cfg.nice, cfg.miss, v);
-    }
-    F[i] = f;
-    G[i] = g;
-    const uint32_t b = __ballot_sync(kAll, f != 0);
-    if (lane == 0) fm[i >> 5] = b;
-  }
-  __syncthreads();
-  for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
-  __syncthreads();
+  uint32_t prev_rs = 0, prev_nreg = 0;
 
-  // -- parse (reference lazy rule, lz77.cpp:449-493, with n = tile end)
-  if (tid == 0) {
-    uint32_t i = 0, nm = 0;
-    while (i < tl) {
-      if (!((fm[i >> 5] >> (i & 31)) & 1u)) {
-        uint32_t w = i >> 5;
-        uint32_t bits = fm[w] & (kAll << (i & 31));
-        while (!bits && ++w < kFmWords) bits = fm[w];
-        if (!bits) break;
-        i = w * 32 + __ffs(bits) - 1;
-        if (i >= tl) break;
+  for (uint32_t ti = first; ti < last; ++ti) {
+    Tile* tp = wk.tiles + ti;
+    const Tile t = *tp;
+    const uint32_t ts = t.start, tl = t.len, tend = ts + tl;
+    const uint32_t rs = ts > W ? ts - W : 0;           // region start (segment-relative)
+    const uint32_t nreg = tend - rs;                    // positions with links
+    const uint32_t copy_end = min(sg.len, tend + 8);    // bytes staged
+    // -- stage bytes [rs, copy_end) at 16-byte granularity
+    const uint64_t g0 = (sg.in_off + rs) & ~uint64_t(15);
+    const uint32_t boff = uint32_t(sg.in_off + rs - g0);
+    const uint32_t n16 = (boff + (copy_end - rs) + 15) / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(wk.in + g0);
+    uint4* dst = reinterpret_cast<uint4*>(sm);
+    for (uint32_t i = tid; i < kDataBytes / 16; i += blockDim.x)
+      dst[i] = i < n16 ? __ldg(src + i) : make_uint4(0, 0, 0, 0);
+    for (uint32_t i = tid; i < 320; i += blockDim.x) hist[i] = 0;
+    // -- carry links and table from the previous tile, or start empty
+    uint32_t lstart = 0;
+    if (ti == first) {
+      for (uint32_t i = tid; i < kTblBytes / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(tbl)[i] = kAll;
+    } else {
+      const uint32_t shift = rs - prev_rs;  // even: tiles and the window are even
+      const uint32_t keep = prev_nreg - shift;
+      uint32_t* lw = reinterpret_cast<uint32_t*>(link);
+      constexpr uint32_t kMaxWords = (kRegion / 2 + 1023) / 1024;
+      uint32_t tmp[kMaxWords];
+#pragma unroll
+      for (uint32_t k = 0; k < kMaxWords; ++k) {
+        const uint32_t wi = tid + k * 1024;
+        tmp[k] = wi * 2 < keep ? lw[wi + shift / 2] : 0u;
       }
-      uint32_t bl = F[i] >> 16, bd = F[i] & 0xFFFFu;
-      int k = cfg.lazy;
-      while (k > 0 && i + bl + 1 < tl && i + 4 <= tl) {
-        const uint32_t g = G[i + 1];
-        if ((g >> 16) > bl + 1) {
-          ++i;
-          bl = g >> 16;
-          bd = g & 0xFFFFu;
-          --k;
-        } else {
-          break;
+      __syncthreads();
+#pragma unroll
+      for (uint32_t k = 0; k < kMaxWords; ++k) {
+        const uint32_t wi = tid + k * 1024;
+        if (wi * 2 < keep) {
+          // a link that now points before the region start is dropped
+          uint32_t lo = tmp[k] & 0xFFFFu, hi = tmp[k] >> 16;
+          if (lo > wi * 2) lo = 0;
+          if (hi > wi * 2 + 1) hi = 0;
+          lw[wi] = lo | (hi << 16);
         }
       }
-      tok_s[i] = 0x80000000u | (bl << 16) | bd;
-      ++nm;
-      i += bl;
+      for (uint32_t i = tid; i < 32768; i += blockDim.x) {
+        const uint32_t e = tbl[i];
+        tbl[i] = (e != 0xFFFFu && e >= shift) ? uint16_t(e - shift) : uint16_t(0xFFFFu);
+      }
+      lstart = keep;
     }
-    scan[63] = nm;
-  }
-  __syncthreads();
+    __syncthreads();
+    const SmemBytes sd{sdata, boff};
 
-  // -- covered bytes (max-scan of match ends) and the histogram
-  const uint32_t per = (T + blockDim.x - 1) / blockDim.x;
-  const uint32_t i0 = tid * per;
-  uint32_t me = 0;
-  for (uint32_t j = 0; j < per; ++j) {
-    const uint32_t i = i0 + j;
-    const uint32_t tk = i < tl ? tok_s[i] : 0;
-    if (tk) me = max(me, i + ((tk >> 16) & 0x1FFu));
-  }
-  const uint32_t nm = scan[63];
-  __syncthreads();
-  uint32_t run = block_max_excl(me, scan);
-  for (uint32_t j = 0; j < per; ++j) {
-    const uint32_t i = i0 + j;
-    if (i >= tl) break;
-    const uint32_t tk = tok_s[i];
-    if (tk) {
-      const uint32_t len = (tk >> 16) & 0x1FFu;
-      atomicAdd(&hist[257 + len_sym(len)], 1u);
-      atomicAdd(&hist[288 + dist_sym(tk & 0xFFFFu)], 1u);
-      run = max(run, i + len);
-    } else if (run <= i) {
-      atomicAdd(&hist[sd.byte(ts - rs + i)], 1u);
+    // -- links of the new positions: previous position with the same 15-bit
+    // hash (warp 0, in order).  32 positions per step; lanes with equal hashes
+    // are found by writing the lane id into dup[h] and reading it back, so
+    // __match_any_sync (slow on distinct values) runs only on clashes.
+    if (wid == 0) {
+      const uint32_t lt = (1u << lane) - 1;
+      for (uint32_t base = lstart; base < nreg; base += 32) {
+        const uint32_t x = base + lane;
+        const bool valid = x < nreg && rs + x + 4 <= sg.len;
+        const uint32_t h = valid ? hash15(sd.load4(x)) : kAll;
+        if (valid) dup[h] = uint8_t(lane);
+        __syncwarp();
+        const bool clash = valid && dup[h] != lane;
+        uint32_t peers = 1u << lane, before = 0;
+        if (__any_sync(kAll, clash)) {
+          peers = __match_any_sync(kAll, h);
+          before = peers & lt;
+        }
+        uint32_t l = 0;
+        if (valid) {
+          const uint32_t pred = before ? base + 31 - __clz(before) : tbl[h];
+          l = pred == 0xFFFFu ? 0u : x - pred;
+        }
+        if (x < nreg) link[x] = uint16_t(l);
+        __syncwarp();
+        if (valid && (peers >> lane) == 1u) tbl[h] = uint16_t(x);
+        __syncwarp();
+      }
     }
-  }
-  __syncthreads();
-  uint32_t* gh = reinterpret_cast<uint32_t*>(wk.scratch + t.hist);
-  for (uint32_t i = tid; i < 320; i += blockDim.x) gh[i] = hist[i];
-  uint32_t* gt = reinterpret_cast<uint32_t*>(wk.scratch + t.tok);
-  for (uint32_t i = tid; i < tl; i += blockDim.x) gt[i] = tok_s[i];
-  if (tid == 0) {
-    tp->fin_matches = nm;
-    tp->fix_bits = 0;
-    tp->splice_bit = 0;
+    if (tid == 0) scan[62] = 0;
+    __syncthreads();
+
+    // -- searches at every tile position; warps take 32-position chunks
+    for (;;) {
+      uint32_t c = 0;
+      if (lane == 0) c = atomicAdd(&scan[62], 1u);
+      c = __shfl_sync(kAll, c, 0);
+      if (c >= kFmWords) break;
+      const uint32_t i = c * 32 + lane;
+      uint32_t f = 0, g = 0;
+      if (i < tl && i + 4 <= tl) {
+        const uint32_t r = ts - rs + i;
+        const uint32_t v = sd.load4(r);
+        const uint32_t maxm = min(258u, tl - i);
+        f = lz_search(sd, link, r, kAll, maxm, cfg.chain, cfg.nice, cfg.miss, v);
+        if (cfg.lazy) g = lz_search(sd, link, r, r - 1, maxm, int(lazy_chain), cfg.nice, cfg.miss, v);
+      }
+      F[i] = f;
+      G[i] = g;
+      const uint32_t b = __ballot_sync(kAll, f != 0);
+      if (lane == 0) fm[c] = b;
+    }
+    for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
+    __syncthreads();
+
+    // -- parse (reference lazy rule, lz77.cpp:449-493, with n = tile end)
+    if (tid == 0) {
+      uint32_t i = 0, nm = 0;
+      while (i < tl) {
+        if (!((fm[i >> 5] >> (i & 31)) & 1u)) {
+          uint32_t w = i >> 5;
+          uint32_t bits = fm[w] & (kAll << (i & 31));
+          while (!bits && ++w < kFmWords) bits = fm[w];
+          if (!bits) break;
+          i = w * 32 + __ffs(bits) - 1;
+          if (i >= tl) break;
+        }
+        uint32_t bl = F[i] >> 16, bd = F[i] & 0xFFFFu;
+        int k = cfg.lazy;
+        while (k > 0 && i + bl + 1 < tl && i + 4 <= tl) {
+          const uint32_t g = G[i + 1];
+          if ((g >> 16) > bl + 1) {
+            ++i;
+            bl = g >> 16;
+            bd = g & 0xFFFFu;
+            --k;
+          } else {
+            break;
+          }
+        }
+        tok_s[i] = 0x80000000u | (bl << 16) | bd;
+        ++nm;
+        i += bl;
+      }
+      scan[63] = nm;
+    }
+    __syncthreads();
+
+    // -- covered bytes (max-scan of match ends) and the histogram
+    const uint32_t per = (T + blockDim.x - 1) / blockDim.x;
+    const uint32_t i0 = tid * per;
+    uint32_t me = 0;
+    for (uint32_t j = 0; j < per; ++j) {
+      const uint32_t i = i0 + j;
+      const uint32_t tk = i < tl ? tok_s[i] : 0;
+      if (tk) me = max(me, i + ((tk >> 16) & 0x1FFu));
+    }
+    const uint32_t nm = scan[63];
+    __syncthreads();
+    uint32_t run = block_max_excl(me, scan);
+    for (uint32_t j = 0; j < per; ++j) {
+      const uint32_t i = i0 + j;
+      if (i >= tl) break;
+      const uint32_t tk = tok_s[i];
+      if (tk) {
+        const uint32_t len = (tk >> 16) & 0x1FFu;
+        atomicAdd(&hist[257 + len_sym(len)], 1u);
+        atomicAdd(&hist[288 + dist_sym(tk & 0xFFFFu)], 1u);
+        run = max(run, i + len);
+      } else if (run <= i) {
+        atomicAdd(&hist[sd.byte(ts - rs + i)], 1u);
+      }
+    }
+    __syncthreads();
+    uint32_t* gh = reinterpret_cast<uint32_t*>(wk.scratch + t.hist);
+    for (uint32_t i = tid; i < 320; i += blockDim.x) gh[i] = hist[i];
+    uint32_t* gt = reinterpret_cast<uint32_t*>(wk.scratch + t.tok);
+    for (uint32_t i = tid; i < tl; i += blockDim.x) gt[i] = tok_s[i];
+    if (tid == 0) {
+      tp->fin_matches = nm;
+      tp->fix_bits = 0;
+      tp->splice_bit = 0;
+    }
+    prev_rs = rs;
+    prev_nreg = nreg;
+    __syncthreads();
   }
 }
 
@@ -628,7 +693,7 @@ __global__ void __launch_bounds__(kEncWarps * 32) k_enc(Work wk, const uint32_t*
 int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms, Marks* mk) {
   if (!L.n_tiles) return 0;
   cudaFuncSetAttribute(k_lz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLz));
-  k_lz<<<L.n_tiles, 1024, kSmemLz, st>>>(wk, L.tiles, L.n_tiles);
+  k_lz<<<L.n_runs, 1024, kSmemLz, st>>>(wk, L.runs, L.n_runs);
   mk->mark(kPhLazyLz, st);
   k_huff<<<(L.n_segs + kHuffWarps - 1) / kHuffWarps, kHuffWarps * 32, 0, st>>>(wk, L.segs, L.n_segs);
   mk->mark(kPhLazyHuff, st);
