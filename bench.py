@@ -22,7 +22,9 @@ Reported (one JSON line from rank 0):
              host cores over a bounded sample;
   serving    Poisson arrivals (2,000 requests/s, 4 KiB-16 MiB, 70% level 1 /
              30% level 6, raw) through the continuous-batching server: p50/p99
-             latency and sustained GB/s, beside the plain path.
+             latency and sustained GB/s; then the server's capacity (the
+             trace submitted at once; mixed, level 1 and level 6) beside the
+             plain path.
 Inputs (5.1 GB) exceed the 126 MB L2, so no flush is needed between steps.
 
 `--impl reference` times the reference's CPU implementation on the same
@@ -236,51 +238,36 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- serving
-def measure_serving(deflate, buf, total, count, rate, seed=0):
-    """Open-loop Poisson arrivals at `rate` requests/s: sizes log-uniform in
-    4 KiB-16 MiB, 70% level 1 / 30% level 6, raw DEFLATE, payloads cut from
-    the mixed workload buffer.  Latency is submission to completion measured
-    by the server; sustained GB/s is the bytes over first submission to last
-    completion.  The same requests, one deflate_compress call at a time, give
-    the plain comparison (on a prefix of the trace)."""
-    from orot_b200 import synth
-    rng = np.random.default_rng(13 + seed)
-    sizes = [int(x) for x in synth.loguniform_sizes(count, 4096, 16 << 20, 13 + seed)]
-    levels = [1 if u < 0.7 else 6 for u in rng.random(count)]
-    starts = [int(rng.integers(0, max(1, total - n))) for n in sizes]
-    gaps = rng.exponential(1.0 / rate, count)
-    caps = [deflate.compress_bound(n, deflate.Format.Raw) for n in sizes]
-    outs = np.empty(sum(caps), np.uint8)
-    ooff = np.concatenate([[0], np.cumsum(caps)])
-    srv = deflate.Server(device_budget=16 << 30, lanes=3)
-    tickets = [0] * count
+def _serve(deflate, srv, buf, trace, gaps):
+    """Submits the trace (arrival gaps in seconds, or None for all at once)
+    and waits for every result; returns latencies (s) and the makespan from
+    first submission to last completion."""
+    sizes, levels, starts, outs, ooff = trace
+    n = len(sizes)
+    tickets = [0] * n
     t0 = time.perf_counter()
     due = t0
-    for i in range(count):
-        due += gaps[i]
-        now = time.perf_counter()
-        if due > now:
-            time.sleep(due - now)
+    for i in range(n):
+        if gaps is not None:
+            due += gaps[i]
+            now = time.perf_counter()
+            if due > now:
+                time.sleep(due - now)
         tickets[i] = srv.submit(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw,
                                 out=outs[ooff[i]:ooff[i + 1]])
     lat = []
-    for i in range(count):
+    for i in range(n):
         o, l = srv.wait(tickets[i], timeout=600)
         if o is None:
             raise SystemExit(f"served request {i} failed")
         lat.append(l)
-    t_end = time.perf_counter()
-    passes, inflight = srv.stats()
-    # spot-check exactness against single calls
-    for i in range(0, count, max(1, count // 25)):
-        ref = deflate.compress(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw)
-        o = outs[ooff[i]:ooff[i] + len(ref)].tobytes()
-        if o != ref:
-            raise SystemExit(f"served request {i} differs from deflate_compress")
-    srv.close()
-    nbytes = sum(sizes)
-    # plain path: the same requests, one deflate_compress at a time
-    k = min(count, 200)
+    return np.array(lat), time.perf_counter() - t0
+
+
+def _plain(deflate, buf, trace, k):
+    """The same requests through deflate_compress, one call after another
+    (service time with no queueing)."""
+    sizes, levels, starts = trace[0], trace[1], trace[2]
     pl = []
     tp = time.perf_counter()
     for i in range(k):
@@ -288,16 +275,63 @@ def measure_serving(deflate, buf, total, count, rate, seed=0):
         deflate.compress(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw)
         pl.append(time.perf_counter() - a)
     tp = time.perf_counter() - tp
-    lat_ms = np.array(lat) * 1e3
-    return {"requests": count, "rate_req_s": rate, "offered_GBps": nbytes / gaps.sum() / 1e9,
-            "sustained_GBps": nbytes / (t_end - t0) / 1e9,
-            "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
-            "passes": passes, "max_passes_in_flight": inflight, "levels": "70% L1 / 30% L6", "format": "raw",
-            "sizes": "log-uniform 4 KiB-16 MiB", "budget_GiB": 16,
-            "plain": {"requests": k, "GBps": sum(sizes[:k]) / tp / 1e9,
-                      "p50_ms": float(np.percentile(np.array(pl) * 1e3, 50)),
-                      "p99_ms": float(np.percentile(np.array(pl) * 1e3, 99)),
-                      "note": "one deflate_compress per request, back to back (service time, no queueing)"}}
+    return {"requests": k, "GBps": sum(sizes[:k]) / tp / 1e9,
+            "p50_ms": float(np.percentile(np.array(pl) * 1e3, 50)),
+            "p99_ms": float(np.percentile(np.array(pl) * 1e3, 99))}
+
+
+def measure_serving(deflate, buf, total, count, rate, seed=0):
+    """Serving: raw DEFLATE requests, sizes log-uniform in 4 KiB-16 MiB, cut
+    from the mixed workload buffer, through the continuous-batching server
+    (16 GiB device budget).
+      open_loop   Poisson arrivals at `rate` requests/s, 70% level 1 / 30%
+                  level 6: p50/p99 latency (submission to completion, timed by
+                  the server) and sustained GB/s (bytes over first submission
+                  to last completion; bounded by the offered rate).
+      capacity    the same trace submitted at once, and the level-1-only and
+                  level-6-only variants: the sustained GB/s the server reaches
+                  when requests queue, beside the plain path (one
+                  deflate_compress per request) on a prefix of the same trace.
+    A sample of served results is checked byte for byte against single
+    deflate_compress calls."""
+    from orot_b200 import synth
+    rng = np.random.default_rng(13 + seed)
+    sizes = [int(x) for x in synth.loguniform_sizes(count, 4096, 16 << 20, 13 + seed)]
+    mix = [1 if u < 0.7 else 6 for u in rng.random(count)]
+    starts = [int(rng.integers(0, max(1, total - n))) for n in sizes]
+    gaps = rng.exponential(1.0 / rate, count)
+    caps = [deflate.compress_bound(n, deflate.Format.Raw) for n in sizes]
+    outs = np.empty(sum(caps), np.uint8)
+    ooff = np.concatenate([[0], np.cumsum(caps)])
+    nbytes = sum(sizes)
+    srv = deflate.Server(device_budget=16 << 30, lanes=3)
+    res = {"requests": count, "rate_req_s": rate, "offered_GBps": nbytes / gaps.sum() / 1e9,
+           "levels": "70% L1 / 30% L6", "format": "raw", "sizes": "log-uniform 4 KiB-16 MiB", "budget_GiB": 16}
+    trace = (sizes, mix, starts, outs, ooff)
+    lat, span = _serve(deflate, srv, buf, trace, gaps)
+    for i in range(0, count, max(1, count // 25)):
+        ref = deflate.compress(buf[starts[i]:starts[i] + sizes[i]], mix[i], deflate.Format.Raw)
+        if outs[ooff[i]:ooff[i] + len(ref)].tobytes() != ref:
+            raise SystemExit(f"served request {i} differs from deflate_compress")
+    lat_ms = lat * 1e3
+    res["open_loop"] = {"sustained_GBps": nbytes / span / 1e9, "p50_ms": float(np.percentile(lat_ms, 50)),
+                        "p99_ms": float(np.percentile(lat_ms, 99))}
+    k = min(count, 200)
+    cap = {}
+    for name, lv in (("mix", mix), ("L1", [1] * count), ("L6", [6] * count)):
+        tr = (sizes, lv, starts, outs, ooff)
+        lat, span = _serve(deflate, srv, buf, tr, None)
+        plain = _plain(deflate, buf, tr, k)
+        cap[name] = {"GBps": nbytes / span / 1e9, "p50_ms": float(np.percentile(lat * 1e3, 50)),
+                     "p99_ms": float(np.percentile(lat * 1e3, 99)), "plain": plain,
+                     "vs_plain": nbytes / span / 1e9 / plain["GBps"]}
+    passes, inflight = srv.stats()
+    srv.close()
+    res["capacity"] = cap
+    res["passes"] = passes
+    res["max_passes_in_flight"] = inflight
+    res["plain_note"] = "one deflate_compress per request, back to back, on the first 200 requests"
+    return res
 
 
 # ---------------------------------------------------------------- GPU arm

@@ -42,10 +42,10 @@ int clamp_level(int l) { return l < 0 ? 0 : l > 12 ? 12 : l; }
 
 bool DevBuf::ensure(size_t n) {
   if (n <= cap) return true;
+  size_t want = std::max(n, cap + cap / 2);  // grow geometrically: cudaFree synchronises the device
   if (p) cudaFree(p);
   p = nullptr;
   cap = 0;
-  size_t want = std::max(n, cap + cap / 2);
   if (cudaMalloc(&p, want) != cudaSuccess) {
     cudaGetLastError();
     if (cudaMalloc(&p, n) != cudaSuccess) { cudaGetLastError(); p = nullptr; set_error("cudaMalloc failed"); return false; }
@@ -58,11 +58,16 @@ void DevBuf::release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
 
 bool HostBuf::ensure(size_t n) {
   if (n <= cap) return true;
+  size_t want = std::max(n, cap + cap / 2);
   if (p) cudaFreeHost(p);
   p = nullptr;
   cap = 0;
-  if (cudaMallocHost(&p, n) != cudaSuccess) { cudaGetLastError(); p = nullptr; set_error("cudaMallocHost failed"); return false; }
-  cap = n;
+  if (cudaMallocHost(&p, want) != cudaSuccess) {
+    cudaGetLastError();
+    if (cudaMallocHost(&p, n) != cudaSuccess) { cudaGetLastError(); p = nullptr; set_error("cudaMallocHost failed"); return false; }
+    want = n;
+  }
+  cap = want;
   return true;
 }
 void HostBuf::release() { if (p) cudaFreeHost(p); p = nullptr; cap = 0; }

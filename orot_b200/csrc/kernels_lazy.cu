@@ -77,44 +77,93 @@ struct SmemBytes {
 __device__ __forceinline__ uint32_t hash16(uint32_t v) { return (v * 0x9E3779B1u) >> 16; }
 __device__ __forceinline__ uint32_t hash15(uint32_t v) { return (v * 0x9E3779B1u) >> 17; }
 
-// Chain search at region position r; returns len << 16 | dist or 0.
-__device__ uint32_t lz_search(const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t r, uint32_t excl,
-                              uint32_t maxm, int chain, int nice, int miss_limit, uint32_t v4p) {
-  const uint32_t h16p = hash16(v4p);
-  uint32_t best = 2, bd = 0, q = r;
-  int steps = chain, misses = 0, budget = 2 * chain + 64;
-  while (budget-- > 0) {
-    const uint32_t l = link[q];
-    if (!l) break;
-    q -= l;
-    if (r - q > 32767u) break;
-    if (q == excl) continue;
-    const uint32_t v = sd.load4(q);
-    if (v != v4p && hash16(v) != h16p) continue;  // same 15-bit bucket, other 16-bit chain
-    if (steps == 0) break;
-    --steps;
-    if (v != v4p) {
-      if (++misses >= miss_limit) break;
-      continue;
-    }
-    misses = 0;
-    // a candidate that differs at byte best cannot beat best (the reference's
-    // quick reject, src/deflate/lz77.cpp:137-142); it changes no result
-    if (best >= 4 && best < maxm && sd.byte(q + best) != sd.byte(r + best)) continue;
-    uint32_t len = 4;
-    while (len < maxm) {
-      const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
-      if (x) { len += (__ffs(x) - 1) >> 3; break; }
-      len += 4;
-    }
-    if (len > maxm) len = maxm;
-    if (len > best) {
-      best = len;
-      bd = r - q;
-      if (int(len) >= nice || len >= maxm) break;  // nothing can beat maxm
-    }
+// The match at r (every candidate, `chain` steps) and the lazy match at r
+// (candidate r - 1 excluded, `gchain` steps) in one walk of the chain: both
+// searches visit the same candidates in the same order, so each follows the
+// single-search rules exactly (hash-16 filter, step and miss limits, the
+// quick reject, early exit at nice or the longest possible length) while the
+// loads and byte comparisons are shared.  The walk advances one candidate per
+// lz_step call so that a lane can start its next position as soon as its
+// chain ends.
+struct LzState {
+  uint32_t r, v4p, h16p, q, maxm;
+  uint32_t bestF, bdF, bestG, bdG;
+  int stepsF, missF, budF, stepsG, missG, budG;
+  bool onF, onG;
+};
+
+__device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, uint32_t r, uint32_t maxm, int chain,
+                                         int gchain) {
+  s.r = r;
+  s.q = r;
+  s.v4p = sd.load4(r);
+  s.h16p = hash16(s.v4p);
+  s.maxm = maxm;
+  s.bestF = s.bestG = 2;
+  s.bdF = s.bdG = 0;
+  s.stepsF = chain;
+  s.budF = 2 * chain + 64;
+  s.stepsG = gchain;
+  s.budG = 2 * gchain + 64;
+  s.missF = s.missG = 0;
+  s.onF = true;
+  s.onG = gchain > 0;
+}
+
+// One candidate; returns true once both searches have ended.
+__device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const uint16_t* __restrict__ link, int nice,
+                                        int miss_limit) {
+  if (s.onF && s.budF-- <= 0) s.onF = false;
+  if (s.onG && s.budG-- <= 0) s.onG = false;
+  if (!s.onF && !s.onG) return true;
+  const uint32_t l = link[s.q];
+  if (!l) return true;
+  s.q -= l;
+  const uint32_t q = s.q, r = s.r;
+  if (r - q > 32767u) return true;
+  bool useF = s.onF, useG = s.onG && q != r - 1;
+  if (!useF && !useG) return false;
+  const uint32_t v = sd.load4(q);
+  if (v != s.v4p && hash16(v) != s.h16p) return false;  // same 15-bit bucket, other 16-bit chain
+  if (useF) {
+    if (s.stepsF == 0) s.onF = useF = false;
+    else --s.stepsF;
   }
-  return best >= 3 ? (best << 16) | bd : 0u;
+  if (useG) {
+    if (s.stepsG == 0) s.onG = useG = false;
+    else --s.stepsG;
+  }
+  if (v != s.v4p) {
+    if (useF && ++s.missF >= miss_limit) s.onF = false;
+    if (useG && ++s.missG >= miss_limit) s.onG = false;
+    return false;
+  }
+  if (useF) s.missF = 0;
+  if (useG) s.missG = 0;
+  // quick reject at byte `best` (src/deflate/lz77.cpp:137-142), per search
+  const uint32_t maxm = s.maxm;
+  const bool needF = useF && !(s.bestF >= 4 && s.bestF < maxm && sd.byte(q + s.bestF) != sd.byte(r + s.bestF));
+  const bool needG = useG && !(s.bestG >= 4 && s.bestG < maxm && sd.byte(q + s.bestG) != sd.byte(r + s.bestG));
+  if (!needF && !needG) return false;
+  uint32_t len = 4;
+  while (len < maxm) {
+    const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
+    if (x) { len += (__ffs(x) - 1) >> 3; break; }
+    len += 4;
+  }
+  if (len > maxm) len = maxm;
+  const bool stop = int(len) >= nice || len >= maxm;
+  if (needF && len > s.bestF) {
+    s.bestF = len;
+    s.bdF = r - q;
+    if (stop) s.onF = false;
+  }
+  if (needG && len > s.bestG) {
+    s.bestG = len;
+    s.bdG = r - q;
+    if (stop) s.onG = false;
+  }
+  return false;
 }
 
 __device__ __forceinline__ uint32_t block_max_excl(uint32_t v, uint32_t* scan) {
@@ -266,24 +315,53 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     if (tid == 0) scan[62] = 0;
     __syncthreads();
 
-    // -- searches at every tile position; warps take 32-position chunks
-    for (;;) {
-      uint32_t c = 0;
-      if (lane == 0) c = atomicAdd(&scan[62], 1u);
-      c = __shfl_sync(kAll, c, 0);
-      if (c >= kFmWords) break;
-      const uint32_t i = c * 32 + lane;
-      uint32_t f = 0, g = 0;
-      if (i < tl && i + 4 <= tl) {
-        const uint32_t r = ts - rs + i;
-        const uint32_t v = sd.load4(r);
-        const uint32_t maxm = min(258u, tl - i);
-        f = lz_search(sd, link, r, kAll, maxm, cfg.chain, cfg.nice, cfg.miss, v);
-        if (cfg.lazy) g = lz_search(sd, link, r, r - 1, maxm, int(lazy_chain), cfg.nice, cfg.miss, v);
+    // -- searches at every tile position.  Warps take 32-position chunks; a
+    // lane whose chain has ended takes the next position of its warp's chunk
+    // at once, so lanes stay busy across chains of very different lengths.
+    {
+      const uint32_t nsearch = tl >= 4 ? tl - 3 : 0;
+      const uint32_t nch = (nsearch + 31) / 32;
+      for (uint32_t i = nsearch + tid; i < kFmWords * 32; i += blockDim.x) F[i] = G[i] = 0;
+      const uint32_t lt = (1u << lane) - 1;
+      const int gchain = cfg.lazy ? int(lazy_chain) : 0;
+      uint32_t pool = 0, avail = 0;  // warp-uniform: next position of the chunk, positions left
+      bool more = true;
+      uint32_t i = kAll;             // this lane's position
+      LzState st;
+      for (;;) {
+        uint32_t idle = __ballot_sync(kAll, i == kAll);
+        while (idle && (avail || more)) {
+          if (!avail) {
+            uint32_t c = 0;
+            if (lane == 0) c = atomicAdd(&scan[62], 1u);
+            c = __shfl_sync(kAll, c, 0);
+            if (c >= nch) {
+              more = false;
+              break;
+            }
+            pool = c * 32;
+            avail = min(32u, nsearch - pool);
+          }
+          const uint32_t take = min(uint32_t(__popc(idle)), avail);
+          if (i == kAll && __popc(idle & lt) < take) {
+            i = pool + __popc(idle & lt);
+            lz_begin(st, sd, ts - rs + i, min(258u, tl - i), cfg.chain, gchain);
+          }
+          pool += take;
+          avail -= take;
+          idle = __ballot_sync(kAll, i == kAll);
+        }
+        if (idle == kAll) break;
+        if (i != kAll && lz_step(st, sd, link, cfg.nice, cfg.miss)) {
+          F[i] = st.bestF >= 3 ? (st.bestF << 16) | st.bdF : 0u;
+          G[i] = st.bestG >= 3 ? (st.bestG << 16) | st.bdG : 0u;
+          i = kAll;
+        }
       }
-      F[i] = f;
-      G[i] = g;
-      const uint32_t b = __ballot_sync(kAll, f != 0);
+    }
+    __syncthreads();
+    for (uint32_t c = wid; c < kFmWords; c += blockDim.x >> 5) {
+      const uint32_t b = __ballot_sync(kAll, F[c * 32 + lane] != 0);
       if (lane == 0) fm[c] = b;
     }
     for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;

@@ -137,6 +137,106 @@ static bool lane_poll(Lane& L, uint64_t cap, bool* failed) {
   return false;
 }
 
+// Runs a pass over synthetic zero bytes so that a lane's host and device
+// arenas reach the size of a full group before traffic arrives (growing them
+// later would free device memory, which waits for every pass in flight).
+static bool lane_warm(Lane& L, uint64_t bytes, int level, uint64_t per_job) {
+  const size_t count = size_t(std::max<uint64_t>(1, bytes / per_job));
+  std::vector<size_t> sz(count, size_t(per_job));
+  std::vector<int> lv(count, level), fm(count, int(DEFLATE_FORMAT_RAW));
+  uint64_t ob = 0;
+  for (size_t i = 0; i < count; ++i) ob += align_up(framed_bound(per_job, 0), 16);
+  if (!L.h_in.ensure(per_job * count) || !L.h_out.ensure(ob + 16)) return false;
+  std::memset(L.h_in.p, 0, per_job * count);
+  L.dst = static_cast<uint8_t*>(L.h_out.p);
+  if (!lane_start(L, static_cast<uint8_t*>(L.h_in.p), sz.data(), lv.data(), fm.data(), nullptr, count)) return false;
+  bool failed = false;
+  while (!lane_poll(L, L.h_out.cap, &failed)) std::this_thread::sleep_for(std::chrono::microseconds(50));
+  return !failed;
+}
+
+// Copies between request memory and pinned staging on a few host threads: one
+// memcpy thread moves about 10 GB/s, below what one pass consumes.
+struct Copy {
+  uint8_t* dst;
+  const uint8_t* src;
+  size_t n;
+};
+
+class CopyPool {
+ public:
+  explicit CopyPool(int n) {
+    for (int i = 0; i < n; ++i) th_.emplace_back([this] { work(); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  // Performs every copy in `v`; returns when all bytes are in place.
+  void run(const std::vector<Copy>& v) {
+    uint64_t total = 0;
+    for (const Copy& c : v) total += c.n;
+    if (th_.empty() || total < kParallelBytes) {
+      for (const Copy& c : v) std::memcpy(c.dst, c.src, c.n);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      chunks_.clear();
+      for (const Copy& c : v)
+        for (size_t o = 0; o < c.n; o += kChunk) chunks_.push_back({c.dst + o, c.src + o, std::min(kChunk, c.n - o)});
+      next_.store(0);
+      done_.store(0);
+      open_ = true;
+      ++gen_;
+    }
+    cv_.notify_all();
+    drain();
+    while (done_.load(std::memory_order_acquire) < chunks_.size()) std::this_thread::yield();
+    std::unique_lock<std::mutex> lk(mu_);
+    open_ = false;
+    cv_idle_.wait(lk, [this] { return busy_ == 0; });
+  }
+
+ private:
+  static constexpr uint64_t kParallelBytes = 4ull << 20;
+  static constexpr size_t kChunk = size_t(1) << 20;
+  void drain() {
+    for (;;) {
+      const size_t i = next_.fetch_add(1);
+      if (i >= chunks_.size()) return;
+      std::memcpy(chunks_[i].dst, chunks_[i].src, chunks_[i].n);
+      done_.fetch_add(1, std::memory_order_release);
+    }
+  }
+  void work() {
+    uint64_t seen = 0;
+    for (;;) {
+      std::unique_lock<std::mutex> lk(mu_);
+      cv_.wait(lk, [&] { return stop_ || (open_ && gen_ != seen); });
+      if (stop_) return;
+      seen = gen_;
+      ++busy_;
+      lk.unlock();
+      drain();
+      lk.lock();
+      if (--busy_ == 0) cv_idle_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, cv_idle_;
+  std::vector<Copy> chunks_;
+  std::atomic<size_t> next_{0}, done_{0};
+  uint64_t gen_ = 0;
+  int busy_ = 0;
+  bool open_ = false, stop_ = false;
+};
+
 // ---------------------------------------------------------------- server
 struct Req {
   uint64_t id;
@@ -163,6 +263,7 @@ struct Server {
   std::thread th;
   int device = 0;
   std::atomic<uint64_t> passes{0}, max_in_flight{0};
+  CopyPool* copies = nullptr;
 
   void run();
 };
@@ -172,22 +273,28 @@ void Server::run() {
   std::vector<int> lv;
   std::vector<int> fm;
   std::vector<size_t> sz, cp;
+  std::vector<Copy> moves;
   while (true) {
     bool progressed = false;
-    // 1. advance lanes in flight
+    // 1. advance lanes in flight; copy finished outputs to their requests
     for (Lane* L : lanes) {
       if (L->state == 0) continue;
       bool failed = false;
       if (!lane_poll(*L, L->h_out.cap, &failed)) continue;
       progressed = true;
-      std::lock_guard<std::mutex> lk(mu);
       const uint64_t* off = L->offsets();
       const uint64_t* s = L->sizes();
+      moves.clear();
+      for (size_t i = 0; !failed && i < L->reqs.size(); ++i) {
+        Req* r = static_cast<Req*>(L->reqs[i]);
+        if (s[i] && s[i] <= r->cap) moves.push_back({r->out, static_cast<uint8_t*>(L->h_out.p) + off[i], size_t(s[i])});
+      }
+      copies->run(moves);
+      std::lock_guard<std::mutex> lk(mu);
       const auto now = Clock::now();
       for (size_t i = 0; i < L->reqs.size(); ++i) {
         Req* r = static_cast<Req*>(L->reqs[i]);
         if (!failed && s[i] && s[i] <= r->cap) {
-          std::memcpy(r->out, static_cast<uint8_t*>(L->h_out.p) + off[i], s[i]);
           r->out_size = s[i];
           r->status = 1;
         } else {
@@ -234,14 +341,16 @@ void Server::run() {
         fm.resize(group.size());
         cp.resize(group.size());
         uint64_t o = 0;
+        moves.clear();
         for (size_t i = 0; ok && i < group.size(); ++i) {
-          std::memcpy(static_cast<uint8_t*>(L->h_in.p) + o, group[i]->in, group[i]->n);
+          moves.push_back({static_cast<uint8_t*>(L->h_in.p) + o, group[i]->in, group[i]->n});
           o += group[i]->n;
           sz[i] = group[i]->n;
           lv[i] = group[i]->level;
           fm[i] = group[i]->fmt;
           cp[i] = group[i]->cap;
         }
+        if (ok) copies->run(moves);
         L->reqs.assign(group.begin(), group.end());
         L->dst = static_cast<uint8_t*>(L->h_out.p);
         if (ok) ok = lane_start(*L, static_cast<uint8_t*>(L->h_in.p), sz.data(), lv.data(), fm.data(), cp.data(),
@@ -288,9 +397,24 @@ deflate_gpu_server* deflate_gpu_server_new(size_t device_budget, int lanes) {
   Server& s = srv->s;
   cudaGetDevice(&s.device);
   s.budget = device_budget ? device_budget : (size_t(16) << 30);
-  s.max_group = std::max<uint64_t>(64ull << 20, s.budget / 16);
   const int nl = lanes > 0 ? std::min(lanes, 8) : 3;
-  for (int i = 0; i < nl; ++i) s.lanes.push_back(new Lane());
+  // Groups of at most 256 MiB keep the queueing delay of a pass to a few ms;
+  // a smaller budget shrinks them so that every lane can hold one.
+  s.max_group = std::min<uint64_t>(256ull << 20, std::max<uint64_t>(16ull << 20, s.budget / (uint64_t(nl) * 10)));
+  for (int i = 0; i < nl; ++i) {
+    Lane* L = new (std::nothrow) Lane();
+    if (!L) break;
+    s.lanes.push_back(L);
+    // size the arenas for a full group: one large lazy-level buffer, then
+    // many small fast-level ones (per-buffer tables)
+    if (!lane_warm(*L, s.max_group, 6, s.max_group) || !lane_warm(*L, s.max_group, 1, 4096)) {
+      for (Lane* X : s.lanes) delete X;
+      delete srv;
+      return nullptr;
+    }
+  }
+  const unsigned hw = std::thread::hardware_concurrency();
+  s.copies = new CopyPool(int(std::min(6u, hw / 4)));
   s.th = std::thread([&s] { s.run(); });
   return srv;
 }
@@ -304,6 +428,7 @@ void deflate_gpu_server_free(deflate_gpu_server* srv) {
   }
   s.cv_work.notify_all();
   if (s.th.joinable()) s.th.join();
+  delete s.copies;
   for (Lane* L : s.lanes) delete L;
   for (auto& kv : s.reqs) delete kv.second;
   delete srv;
