@@ -44,8 +44,7 @@ constexpr uint32_t kRegion = W + T;                            // positions with
 constexpr uint32_t kDataBytes = (W + T + 48 + 127) / 128 * 128;  // + align + over-read tail
 constexpr uint32_t kLinkBytes = (kRegion * 2 + 127) / 128 * 128;  // u16 per position
 constexpr uint32_t kTblBytes = 65536;                          // u16 per 15-bit hash, kept across a run
-constexpr uint32_t kDupBytes = 1u << 15;                       // u8 per 15-bit hash (link construction)
-constexpr uint32_t kFgBytes = T * 8 > kDupBytes ? T * 8 : kDupBytes;  // F[T] + G[T], aliasing dup
+constexpr uint32_t kFgBytes = T * 8;                           // F[T] + G[T]; link marks before the search
 constexpr uint32_t kTokBytes = T * 4;
 constexpr uint32_t kFmWords = T / 32;
 constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFgBytes + kTokBytes + kFmWords * 4 + 320 * 4 +
@@ -53,6 +52,9 @@ constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFgBytes + kT
 static_assert(T % 32 == 0, "tiles are whole windows of 32 positions");
 static_assert(kSmemLz <= 227 * 1024, "one CTA per SM");
 static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words of links");
+static_assert((kRegion + 31) / 32 * 8 <= kFgBytes, "first/last marks of every link chunk fit F");
+
+constexpr uint32_t kSerialParse = 128;  // at most this many match positions: serial parse
 
 struct LazyCfg { int chain, nice, lazy, miss; };
 __constant__ LazyCfg c_lazy[13] = {
@@ -166,6 +168,44 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
   return false;
 }
 
+// First position >= i where a match starts (a set bit of fm), or tl.
+__device__ __forceinline__ uint32_t next_head(const uint32_t* fm, uint32_t i, uint32_t tl) {
+  if (i >= tl) return tl;
+  uint32_t w = i >> 5;
+  uint32_t bits = fm[w] & (kAll << (i & 31));
+  while (!bits && ++w < (tl + 31) / 32) bits = fm[w];
+  return bits ? min(w * 32 + __ffs(bits) - 1, tl) : tl;
+}
+
+// One step of the lazy parse from head i (F[i] != 0): up to `lazy` moves to
+// i + 1 while the lazy match there is longer by two or more.  Returns
+// {match position, len << 16 | dist}.
+__device__ __forceinline__ uint2 lazy_step(const uint32_t* F, const uint32_t* G, uint32_t i, uint32_t tl, int lazy) {
+  uint32_t m = F[i];
+  int k = lazy;
+  while (k > 0 && i + (m >> 16) + 1 < tl && i + 4 <= tl) {
+    const uint32_t g = G[i + 1];
+    if ((g >> 16) > (m >> 16) + 1) {
+      ++i;
+      m = g;
+      --k;
+    } else {
+      break;
+    }
+  }
+  return make_uint2(i, m);
+}
+
+// Clears the bits of positions [lo, hi).
+__device__ __forceinline__ void clear_bits(uint32_t* bm, uint32_t lo, uint32_t hi) {
+  while (lo < hi) {
+    const uint32_t w = lo >> 5, b0 = lo & 31, n = min(32u - b0, hi - lo);
+    const uint32_t mask = (n == 32 ? kAll : ((1u << n) - 1)) << b0;
+    bm[w] &= ~mask;
+    lo += n;
+  }
+}
+
 __device__ __forceinline__ uint32_t block_max_excl(uint32_t v, uint32_t* scan) {
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   uint32_t inc = v;
@@ -216,7 +256,6 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
   uint8_t* fgb = sm + kDataBytes + kLinkBytes + kTblBytes;
   uint32_t* F = reinterpret_cast<uint32_t*>(fgb);
   uint32_t* G = F + T;
-  uint8_t* dup = fgb;  // only while linking
   uint32_t* tok_s = reinterpret_cast<uint32_t*>(fgb + kFgBytes);
   uint32_t* fm = tok_s + T;
   uint32_t* hist = fm + kFmWords;
@@ -283,33 +322,61 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     __syncthreads();
     const SmemBytes sd{sdata, boff};
 
-    // -- links of the new positions: previous position with the same 15-bit
-    // hash (warp 0, in order).  32 positions per step; lanes with equal hashes
-    // are found by writing the lane id into dup[h] and reading it back, so
-    // __match_any_sync (slow on distinct values) runs only on clashes.
-    if (wid == 0) {
+    // -- links of the new positions [lstart, nreg): the previous position
+    // with the same 15-bit hash.  (1) All warps, 32-position chunks: the
+    // nearest earlier lane with the same hash is the link inside the chunk,
+    // and the first and last lane of every hash are marked.  (2) Warp 0,
+    // chunk after chunk: first lanes link to the table's position, last
+    // lanes replace it.  Only step (2) is sequential, and it does one table
+    // read and one table write per distinct hash.
+    {
+      const uint32_t nch = (nreg - lstart + 31) / 32;
+      uint32_t* fbits = F;  // F/G are free until the searches
+      uint32_t* lbits = F + nch;
       const uint32_t lt = (1u << lane) - 1;
-      for (uint32_t base = lstart; base < nreg; base += 32) {
-        const uint32_t x = base + lane;
+      for (uint32_t c = wid; c < nch; c += blockDim.x >> 5) {
+        const uint32_t x = lstart + c * 32 + lane;
         const bool valid = x < nreg && rs + x + 4 <= sg.len;
-        const uint32_t h = valid ? hash15(sd.load4(x)) : kAll;
-        if (valid) dup[h] = uint8_t(lane);
-        __syncwarp();
-        const bool clash = valid && dup[h] != lane;
-        uint32_t peers = 1u << lane, before = 0;
-        if (__any_sync(kAll, clash)) {
-          peers = __match_any_sync(kAll, h);
-          before = peers & lt;
+        const uint32_t h = valid ? hash15(sd.load4(x)) : 0x10000u + lane;  // invalid lanes match nobody
+        const uint32_t peers = __match_any_sync(kAll, h);
+        const uint32_t before = peers & lt;
+        if (x < nreg) link[x] = before ? uint16_t(__clz(before) - (31 - lane)) : uint16_t(0);
+        const uint32_t first = __ballot_sync(kAll, valid && !before);
+        const uint32_t last = __ballot_sync(kAll, valid && !(peers & ~lt & ~(1u << lane)));
+        if (lane == 0) {
+          fbits[c] = first;
+          lbits[c] = last;
         }
-        uint32_t l = 0;
-        if (valid) {
-          const uint32_t pred = before ? base + 31 - __clz(before) : tbl[h];
-          l = pred == 0xFFFFu ? 0u : x - pred;
+      }
+      __syncthreads();
+      if (wid == 0) {
+        // eight chunks per round: their marks and hashes are loaded first,
+        // then the table reads and writes go in chunk order without waiting
+        // for each other's results
+        constexpr uint32_t U = 8;
+        for (uint32_t c0 = 0; c0 < nch; c0 += U) {
+          uint32_t fb[U], lb[U], h[U], p[U];
+#pragma unroll
+          for (uint32_t u = 0; u < U; ++u) {
+            fb[u] = c0 + u < nch ? (fbits[c0 + u] >> lane) & 1u : 0u;
+            lb[u] = c0 + u < nch ? (lbits[c0 + u] >> lane) & 1u : 0u;
+          }
+#pragma unroll
+          for (uint32_t u = 0; u < U; ++u)
+            h[u] = (fb[u] | lb[u]) ? hash15(sd.load4(lstart + (c0 + u) * 32 + lane)) : 0u;
+#pragma unroll
+          for (uint32_t u = 0; u < U; ++u) {
+            p[u] = fb[u] ? uint32_t(tbl[h[u]]) : 0xFFFFu;
+            __syncwarp();
+            if (lb[u]) tbl[h[u]] = uint16_t(lstart + (c0 + u) * 32 + lane);
+            __syncwarp();
+          }
+#pragma unroll
+          for (uint32_t u = 0; u < U; ++u) {
+            const uint32_t x = lstart + (c0 + u) * 32 + lane;
+            if (fb[u]) link[x] = p[u] == 0xFFFFu ? uint16_t(0) : uint16_t(x - p[u]);
+          }
         }
-        if (x < nreg) link[x] = uint16_t(l);
-        __syncwarp();
-        if (valid && (peers >> lane) == 1u) tbl[h] = uint16_t(x);
-        __syncwarp();
       }
     }
     if (tid == 0) scan[62] = 0;
@@ -367,36 +434,89 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
     __syncthreads();
 
-    // -- parse (reference lazy rule, lz77.cpp:449-493, with n = tile end)
-    if (tid == 0) {
-      uint32_t i = 0, nm = 0;
-      while (i < tl) {
-        if (!((fm[i >> 5] >> (i & 31)) & 1u)) {
-          uint32_t w = i >> 5;
-          uint32_t bits = fm[w] & (kAll << (i & 31));
-          while (!bits && ++w < kFmWords) bits = fm[w];
-          if (!bits) break;
-          i = w * 32 + __ffs(bits) - 1;
-          if (i >= tl) break;
-        }
-        uint32_t bl = F[i] >> 16, bd = F[i] & 0xFFFFu;
-        int k = cfg.lazy;
-        while (k > 0 && i + bl + 1 < tl && i + 4 <= tl) {
-          const uint32_t g = G[i + 1];
-          if ((g >> 16) > bl + 1) {
-            ++i;
-            bl = g >> 16;
-            bd = g & 0xFFFFu;
-            --k;
-          } else {
-            break;
+    // -- parse (reference lazy rule, lz77.cpp:449-493, with n = tile end).
+    // A parse step depends only on its start position (the head), so the
+    // heads are found in parallel: (1) each lane of warp 0 parses one 1/32 of
+    // the tile from its start; (2) lane 0 follows the true parse into every
+    // segment until it meets a head of that segment's parse, after which the
+    // two are the same; (3) every thread emits the matches of its heads.
+    {
+      uint32_t* hd = hist;  // heads, a bit per position (hist is zero until the histogram)
+      uint32_t* sx = scan;  // where each segment's parse leaves it
+      const uint32_t S = (tl + 31) / 32;
+      uint32_t nf = 0;  // positions with a match: few -> one lane parses alone
+      if (wid == 0) {
+        for (uint32_t w = lane; w < kFmWords; w += 32) nf += __popc(fm[w]);
+        nf = __reduce_add_sync(kAll, nf);
+      }
+      if (wid == 0 && nf <= kSerialParse) {
+        if (lane == 0) {
+          uint32_t i = 0;
+          while ((i = next_head(fm, i, tl)) < tl) {
+            hd[i >> 5] |= 1u << (i & 31);
+            const uint2 m = lazy_step(F, G, i, tl, cfg.lazy);
+            i = (m.x & 0xFFFFu) + (m.y >> 16);
           }
         }
-        tok_s[i] = 0x80000000u | (bl << 16) | bd;
-        ++nm;
-        i += bl;
+      } else if (wid == 0) {
+        const uint32_t a = min(lane * S, tl), b = min(a + S, tl);
+        uint32_t i = a;
+        while (i < b) {
+          i = next_head(fm, i, tl);
+          if (i >= b) break;
+          atomicOr(&hd[i >> 5], 1u << (i & 31));
+          const uint2 m = lazy_step(F, G, i, tl, cfg.lazy);
+          i = (m.x & 0xFFFFu) + (m.y >> 16);
+        }
+        sx[lane] = i;
+        __syncwarp();
+        if (lane == 0) {
+          uint32_t e = sx[0];
+          for (uint32_t sgi = 1; sgi < 32; ++sgi) {
+            const uint32_t a2 = min(sgi * S, tl), b2 = min(a2 + S, tl);
+            if (a2 >= b2) break;
+            clear_bits(hd, a2, min(e, b2));
+            if (e >= b2) continue;
+            uint32_t i2 = e;
+            for (;;) {
+              const uint32_t h = next_head(fm, i2, tl);
+              if (h >= b2) {
+                e = h;
+                break;
+              }
+              if ((hd[h >> 5] >> (h & 31)) & 1u) {
+                e = sx[sgi];
+                break;
+              }
+              hd[h >> 5] |= 1u << (h & 31);
+              const uint2 m = lazy_step(F, G, h, tl, cfg.lazy);
+              i2 = (m.x & 0xFFFFu) + (m.y >> 16);
+              clear_bits(hd, h + 1, min(i2, b2));
+              if (i2 >= b2) {
+                e = i2;
+                break;
+              }
+            }
+          }
+        }
       }
-      scan[63] = nm;
+      __syncthreads();
+      for (uint32_t i = tid; i < tl; i += blockDim.x) {
+        if ((hd[i >> 5] >> (i & 31)) & 1u) {
+          const uint2 m = lazy_step(F, G, i, tl, cfg.lazy);
+          tok_s[m.x & 0xFFFFu] = 0x80000000u | m.y;
+        }
+      }
+      __syncthreads();
+      if (wid == 0) {
+        uint32_t nm = 0;
+        for (uint32_t w = lane; w < kFmWords; w += 32) {
+          nm += __popc(hd[w]);
+          hd[w] = 0;
+        }
+        nm = __reduce_add_sync(kAll, nm);
+        if (lane == 0) scan[63] = nm;
+      }
     }
     __syncthreads();
 
