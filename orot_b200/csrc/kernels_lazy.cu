@@ -142,11 +142,14 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
   }
   if (useF) s.missF = 0;
   if (useG) s.missG = 0;
-  // quick reject at byte `best` (src/deflate/lz77.cpp:137-142), per search
+  // quick reject (src/deflate/lz77.cpp:137-142): a search improves only on
+  // a candidate whose first best + 1 bytes all match, so 4 bytes ending at
+  // the smaller best of the searches still open decide for both; a
+  // candidate let through here is measured and cannot change a result
   const uint32_t maxm = s.maxm;
-  const bool needF = useF && !(s.bestF >= 4 && s.bestF < maxm && sd.byte(q + s.bestF) != sd.byte(r + s.bestF));
-  const bool needG = useG && !(s.bestG >= 4 && s.bestG < maxm && sd.byte(q + s.bestG) != sd.byte(r + s.bestG));
-  if (!needF && !needG) return false;
+  const uint32_t mb = min(useF ? s.bestF : 0xFFFFu, useG ? s.bestG : 0xFFFFu);
+  if (mb >= 4 && mb < maxm && sd.load4(q + mb - 3) != sd.load4(r + mb - 3)) return false;
+  const bool needF = useF, needG = useG;
   uint32_t len = 4;
   while (len < maxm) {
     const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
