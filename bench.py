@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     return ap.parse_args()
 
 
@@ -476,7 +477,7 @@ def main():
             raise SystemExit("end-to-end sizes differ from the device-resident pass")
         e2e = {"value": world * total / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": total,
                "d2h_bytes_per_step": int(comp) + 16 * (len(sizes) + 1), "ms_per_step": dt * 1e3,
-               "api": "deflate_gpu_compress_pipelined (pinned host buffers, 512 MiB groups, 3 passes in flight)"}
+               "api": "deflate_gpu_compress_pipelined (pinned host buffers, 512 MiB groups, 4 passes in flight)"}
 
     # -- serving: Poisson arrivals through the continuous-batching server
     serving = None
@@ -485,7 +486,7 @@ def main():
 
     # -- CPU baseline: the reference on the host cores (rank 0, N = 1 only)
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
         idx = sample_indices(sizes, 1 << 30, 21)
         r, nb, dt, cratio, kind = cpu_sample_rate(buf, sizes, offs, idx, args.level, threads)

@@ -220,6 +220,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
         c.in_off = j.in_off + o;
         c.len = uint32_t(std::min<uint64_t>(65536, j.in_len - o));
         c.stream = uint32_t(ji);
+        c.what = j.fmt == kFmtGzip ? kCkCrc : kCkAdler;
         cks.push_back(c);
       }
     }
@@ -406,6 +407,7 @@ uint32_t Engine::checksum_host(uint32_t init, const void* data, size_t n, bool a
     CkBlock c{};
     c.in_off = o;
     c.len = uint32_t(std::min<uint64_t>(65536, n - o));
+    c.what = adler ? kCkAdler : kCkCrc;
     cks.push_back(c);
   }
   const size_t ck_bytes = cks.size() * sizeof(CkBlock);

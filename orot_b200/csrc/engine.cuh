@@ -113,8 +113,9 @@ struct CkBlock {
   uint32_t stream;
   uint32_t crc;        // raw CRC register from 0 (no conditioning)
   uint32_t a, b;       // Adler partial sums mod 65521
-  uint32_t pad;
+  uint32_t what;       // kCkCrc | kCkAdler: the sums the stream needs
 };
+constexpr uint32_t kCkCrc = 1u, kCkAdler = 2u;
 
 // Limits.
 constexpr int kMaxTileLog2 = 16;           // 64 KiB tiles at most

@@ -166,21 +166,34 @@ __global__ void __launch_bounds__(256) k_ck_block(Work wk, CrcPowers pw) {
   const uint8_t* p = wk.in + b.in_off + o0;
   uint32_t crc = 0, A = 0, B = 0;
   uint32_t i = 0;
-  // aligned words, funnel-shifted when the block does not start on a word
+  const uint32_t what = b.what;  // uniform over the block
+  // one 32-bit word: CRC slicing-by-4; Adler A += bytes, B += 4A + 4,3,2,1-weighted bytes
+  auto word = [&](uint32_t v) {
+    if (what & kCkCrc) {
+      crc ^= v;
+      crc = tb[3][crc & 0xFF] ^ tb[2][(crc >> 8) & 0xFF] ^ tb[1][(crc >> 16) & 0xFF] ^ tb[0][crc >> 24];
+    }
+    if (what & kCkAdler) {
+      B += 4 * A + __dp4a(v, 0x01020304u, 0u);
+      A += __dp4a(v, 0x01010101u, 0u);
+    }
+  };
   const uint64_t ab = b.in_off + o0;
-  const uint32_t* pw4 = reinterpret_cast<const uint32_t*>(wk.in + (ab & ~uint64_t(3)));
-  const uint32_t sh = uint32_t(ab & 3) * 8;
-  for (; i + 4 <= len; i += 4) {
-    const uint32_t v = sh ? __funnelshift_r(__ldg(pw4 + (i >> 2)), __ldg(pw4 + (i >> 2) + 1), sh) : __ldg(pw4 + (i >> 2));
-    crc ^= v;
-    crc = tb[3][crc & 0xFF] ^ tb[2][(crc >> 8) & 0xFF] ^ tb[1][(crc >> 16) & 0xFF] ^ tb[0][crc >> 24];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const uint32_t by = (v >> (8 * k)) & 0xFF;
-      A += by;
-      B += A;
+  if ((ab & 15) == 0) {
+    const uint4* p16 = reinterpret_cast<const uint4*>(wk.in + ab);
+    for (; i + 16 <= len; i += 16) {
+      const uint4 v = __ldg(p16 + (i >> 4));
+      word(v.x);
+      word(v.y);
+      word(v.z);
+      word(v.w);
     }
   }
+  // aligned words, funnel-shifted when the block does not start on a word
+  const uint32_t* pw4 = reinterpret_cast<const uint32_t*>(wk.in + (ab & ~uint64_t(3)));
+  const uint32_t sh = uint32_t(ab & 3) * 8;
+  for (; i + 4 <= len; i += 4)
+    word(sh ? __funnelshift_r(__ldg(pw4 + (i >> 2)), __ldg(pw4 + (i >> 2) + 1), sh) : __ldg(pw4 + (i >> 2)));
   for (; i < len; ++i) {
     const uint32_t by = p[i];
     crc = tb[0][(crc ^ by) & 0xFF] ^ (crc >> 8);
@@ -198,10 +211,14 @@ __global__ void __launch_bounds__(256) k_ck_block(Work wk, CrcPowers pw) {
     if ((t & (2 * s - 1)) == 0 && t + s < 256) {
       const uint32_t lr = sl[t + s];
       if (lr) {
-        const uint32_t shift = (lr == kCkSub * s) ? c_crc_sub[lvl] : xpow8n(pw, lr);
-        sc[t] = gf2_mulmod(shift, sc[t]) ^ sc[t + s];
-        sb2[t] = uint32_t((uint64_t(sb2[t]) + uint64_t(lr % kAdlerMod) * sa[t] + sb2[t + s]) % kAdlerMod);
-        sa[t] = (sa[t] + sa[t + s]) % kAdlerMod;
+        if (what & kCkCrc) {
+          const uint32_t shift = (lr == kCkSub * s) ? c_crc_sub[lvl] : xpow8n(pw, lr);
+          sc[t] = gf2_mulmod(shift, sc[t]) ^ sc[t + s];
+        }
+        if (what & kCkAdler) {
+          sb2[t] = uint32_t((uint64_t(sb2[t]) + uint64_t(lr % kAdlerMod) * sa[t] + sb2[t + s]) % kAdlerMod);
+          sa[t] = (sa[t] + sa[t + s]) % kAdlerMod;
+        }
         sl[t] += lr;
       }
     }

@@ -497,7 +497,7 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
   if (!count || !in_sizes || !out_packed || !out_offsets || !out_sizes || int(format) < 0 || int(format) > 2) return 0;
   std::lock_guard<std::mutex> lk(global_mutex());
   static std::vector<Lane*> pool;
-  const int nl = lanes > 0 ? std::min(lanes, 8) : 3;
+  const int nl = lanes > 0 ? std::min(lanes, 8) : 4;
   while (int(pool.size()) < nl) pool.push_back(new Lane());
   if (!group_bytes) group_bytes = size_t(512) << 20;
   // groups: contiguous buffer ranges
