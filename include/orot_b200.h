@@ -185,6 +185,26 @@ int deflate_gpu_server_wait(deflate_gpu_server* s, uint64_t ticket, size_t* out_
                             double timeout_s);
 int deflate_gpu_server_stats(deflate_gpu_server* s, uint64_t* passes, uint64_t* max_in_flight);
 
+/* One pigz-style stream compressed by several GPUs (no counterpart in the
+ * reference; the unit it shards is the chunk of deflate_parallel_compress,
+ * src/parallel/parallel_compressor.cpp:36-150).  The input is split into
+ * contiguous ranges of whole block_size chunks, one per rank; each rank
+ * compresses its range into a bare part: raw DEFLATE with no header or
+ * trailer, ending with an empty stored block (sync point) unless it is the
+ * final part, which carries BFINAL.  The stream is the header of `format`,
+ * the parts in rank order and the trailer built from the combined checksum
+ * and the total length.  *checksum receives the range's Adler-32 (zlib),
+ * CRC-32 (gzip) or 0 (raw).  A rank with no chunks passes in_size 0 and
+ * final_part 0 and gets an empty part.  Returns 0, -1 bad argument,
+ * -2 device failure, -3 out_capacity too small (deflate_compress_bound() of
+ * the range always suffices). */
+int deflate_gpu_parallel_shard(const void* in, size_t in_size, int level, deflate_format format, size_t block_size,
+                               int final_part, void* out, size_t out_capacity, size_t* out_size, uint32_t* checksum);
+/* crc32(A||B) from crc32(A), crc32(B) and |B| (zlib's crc32_combine). */
+uint32_t deflate_crc32_combine(uint32_t crc1, uint32_t crc2, uint64_t len2);
+/* adler32(A||B) from adler32(A), adler32(B) and |B| (zlib's adler32_combine). */
+uint32_t deflate_adler32_combine(uint32_t adler1, uint32_t adler2, uint64_t len2);
+
 /* No-allocation variant (no counterpart in the reference).  For callers that
  * own every byte of device memory and cannot let a library call cudaMalloc
  * (a host framework's pool allocator, a fixed device-memory budget): inputs,

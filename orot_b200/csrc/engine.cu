@@ -132,6 +132,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
     s.level = j.level;
     s.fmt = uint32_t(j.fmt);
     s.parallel = j.parallel ? 1 : 0;
+    s.mode = j.mode;
     s.seg_first = uint32_t(segs.size());
     s.piece_first = npieces;
     const int lv = clamp_level(j.level);
@@ -146,7 +147,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
       g.len = uint32_t(len);
       g.stream = uint32_t(ji);
       g.level = lv;
-      g.flags = (k + 1 == nseg ? kSegLast : 0) | (j.parallel ? 0 : kSegWholeBuf);
+      g.flags = (k + 1 == nseg && !(j.mode & kStreamOpen) ? kSegLast : 0) | (j.parallel ? 0 : kSegWholeBuf);
       g.tile_first = uint32_t(tiles.size());
       const int hb = lv <= 0 ? 0 : lv == 1 ? 12 : lv <= 3 ? 14 : 0;
       const uint32_t H = hb ? (1u << hb) : 0;
@@ -212,6 +213,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
       segs.push_back(g);
     }
     s.seg_count = uint32_t(segs.size()) - s.seg_first;
+    if (j.mode & kStreamOpen) npieces += 2;  // the closing sync point
     s.piece_count = npieces - s.piece_first;
     s.ck_first = uint32_t(cks.size());
     if (j.fmt != kFmtRaw) {
@@ -369,7 +371,7 @@ size_t parallel_bound(size_t n, int fmt, int level, size_t block) {
 }
 
 size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel,
-                             size_t block) {
+                             size_t block, uint32_t mode, Stream* result) {
   const size_t bound = parallel ? parallel_bound(n, fmt, level, block) : framed_bound(n, fmt);
   if (!ensure_io(align_up(n, 16), align_up(bound, 16))) return 0;
   if (n) {
@@ -378,7 +380,7 @@ size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, in
     if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) { set_error("H2D failed"); return 0; }
   }
   std::vector<Job> jobs(1);
-  jobs[0] = Job{0, n, 0, parallel ? std::min<uint64_t>(cap, bound) : bound, level, fmt, parallel, block};
+  jobs[0] = Job{0, n, 0, parallel ? std::min<uint64_t>(cap, bound) : bound, level, fmt, parallel, block, mode};
   if (!plan(jobs) || !launch(stream)) return 0;
   Stream s{};
   if (cudaMemcpyAsync(&s, static_cast<uint8_t*>(d_tables.p) + off_streams, sizeof s, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
@@ -386,6 +388,7 @@ size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, in
     set_error(std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
     return 0;
   }
+  if (result) *result = s;
   if (s.error || s.out_size == 0 || s.out_size > cap) return 0;
   if (!h_stage.ensure(s.out_size)) return 0;
   if (cudaMemcpyAsync(h_stage.p, static_cast<uint8_t*>(d_out.p) + s.out_off, s.out_size, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||

@@ -38,11 +38,19 @@ struct Stream {
   uint32_t fmt;
   uint32_t parallel;   // 1: pigz framing (gzip XFL = 0)
   uint32_t ck_first, ck_count;  // checksum blocks of this stream
+  uint32_t mode;       // kStreamBare | kStreamOpen
+  uint32_t pad2;
   // results
   uint64_t out_size;   // framed bytes, 0 on error
+  uint64_t raw_bits;   // bits of the raw DEFLATE part
   uint32_t checksum;
   uint32_t error;
 };
+// Stream modes for one rank's part of a stream compressed across GPUs:
+// Bare: no header or trailer (the checksum of fmt is still computed);
+// Open: another part follows, so no block is BFINAL and the part ends with an
+// empty stored block, a sync point that leaves it on a byte boundary.
+constexpr uint32_t kStreamBare = 1u, kStreamOpen = 2u;
 
 struct Segment {
   uint64_t in_off;     // absolute byte offset in the input arena

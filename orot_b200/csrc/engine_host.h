@@ -41,6 +41,7 @@ struct Job {
   int fmt;
   bool parallel;        // pigz chunking instead of one block per buffer
   uint64_t block_size;  // chunk size for parallel (0 = by level)
+  uint32_t mode = 0;    // kStreamBare | kStreamOpen
 };
 
 enum ListId {
@@ -61,7 +62,10 @@ class Engine {
   bool plan(const std::vector<Job>& jobs);
   bool launch(cudaStream_t st);
   Work work() const;
-  size_t compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel, size_t block);
+  // One stream from host memory to host memory; `mode` takes kStreamBare /
+  // kStreamOpen and `result` (optional) receives the stream's table entry.
+  size_t compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel, size_t block,
+                       uint32_t mode = 0, Stream* result = nullptr);
   uint32_t checksum_host(uint32_t init, const void* data, size_t n, bool adler);
   uint32_t pick_tile(uint64_t total_bytes) const;
 

@@ -38,7 +38,8 @@ __global__ void k_plan(Work wk) {
   const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
   if (si >= wk.nstreams) return;
   Stream s = wk.streams[si];
-  const uint32_t hdr = fmt_header_bytes(s.fmt), trl = fmt_trailer_bytes(s.fmt);
+  const bool bare = (s.mode & kStreamBare) != 0;
+  const uint32_t hdr = bare ? 0 : fmt_header_bytes(s.fmt), trl = bare ? 0 : fmt_trailer_bytes(s.fmt);
   uint32_t* dst = reinterpret_cast<uint32_t*>(wk.out + s.out_off);
   Piece* pc = wk.pieces + s.piece_first;
   uint32_t k = 0;
@@ -121,8 +122,16 @@ __global__ void k_plan(Work wk) {
     sg.bits = c - start;
     wk.segs[g] = sg;
   }
+  if (s.mode & kStreamOpen) {
+    // sync point: empty stored block, BFINAL = 0, LEN 0000 NLEN FFFF
+    put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 3, 0u);
+    c = (c + 3 + 7) & ~uint64_t(7);
+    put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 32, 0xFFFF0000u);
+    c += 32;
+  }
   bad = k > kmax;
   const uint64_t size = uint64_t(hdr) + c / 8 + trl;
+  s.raw_bits = c;
   s.error = kErrNone;
   if (bad) s.error = kErrInternal;
   else if (size > s.out_cap) s.error = kErrCapacity;
@@ -322,7 +331,7 @@ __global__ void k_frame(Work wk) {
   const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
   if (si >= wk.nstreams) return;
   const Stream s = wk.streams[si];
-  if (s.error || s.fmt == kFmtRaw) return;
+  if (s.error || s.fmt == kFmtRaw || (s.mode & kStreamBare)) return;
   uint8_t* o = wk.out + s.out_off;
   const uint64_t end = s.out_size;
   if (s.fmt == kFmtZlib) {

@@ -110,6 +110,13 @@ def lib() -> ctypes.CDLL:
                                           c.c_double]
     L.deflate_gpu_server_stats.restype = c.c_int
     L.deflate_gpu_server_stats.argtypes = [c.c_void_p, c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
+    L.deflate_gpu_parallel_shard.restype = c.c_int
+    L.deflate_gpu_parallel_shard.argtypes = [c.c_void_p, c.c_size_t, c.c_int, c.c_int, c.c_size_t, c.c_int, c.c_void_p,
+                                             c.c_size_t, c.POINTER(c.c_size_t), c.POINTER(c.c_uint32)]
+    L.deflate_crc32_combine.restype = c.c_uint32
+    L.deflate_crc32_combine.argtypes = [c.c_uint32, c.c_uint32, c.c_uint64]
+    L.deflate_adler32_combine.restype = c.c_uint32
+    L.deflate_adler32_combine.argtypes = [c.c_uint32, c.c_uint32, c.c_uint64]
     _lib = L
     return L
 
