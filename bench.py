@@ -53,9 +53,11 @@ METRIC = "deflate_compress_GBps_batched"
 UNIT = "GB/s"
 WORKLOAD = "10000 zlib buffers, log-uniform 1 KiB-4 MiB, mixed text/ints/zeros/random, level 1, one pass"
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes per input byte of the fast-level walk phase, from the ncu capture
-# summarised in profiles/k_walk_mixed.md (read + write, scaled per input byte).
-WALK_DRAM_BYTES_PER_INPUT_BYTE = None
+# DRAM bytes (read + write) per input byte of the walk kernel, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on the first 600 buffers of
+# this workload (301.5 MB): 588 MB + 848 MB.  Every term of that traffic is per
+# byte or per tile, so it is scaled by the input size for the full launch.
+WALK_DRAM_BYTES_PER_INPUT_BYTE = (588.288256e6 + 847.898624e6) / 301540590
 
 
 def parse():

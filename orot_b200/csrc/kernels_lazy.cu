@@ -10,20 +10,22 @@
 // GPU-native differences, all keeping the stream valid:
 //   * a chain ends at the 32 KiB window edge (the reference keeps walking
 //     with distances taken mod 32768);
-//   * the input is cut into independent 8 KiB tiles: each tile parses from
-//     its own first byte and matches do not run past its end, while still
-//     referencing up to 32 KiB before the tile;
+//   * the input is cut into independent 4 KiB tiles (16 x 258 bytes): each
+//     tile parses from its own first byte and matches do not run past its
+//     end, while still referencing up to 32 KiB before the tile;
 //   * levels 10-12 use the same chains with 1024/2048/4096 steps and lazy
 //     depth 3 instead of the reference's binary tree;
 //   * code lengths come from an optimal two-queue Huffman construction with
 //     the ITU-T T.81 Annex K.3 length limiter, and the block type is chosen
 //     on exact sizes (the reference uses a flat header estimate).
 //
-//   k_lz     one CTA per tile: stage the window + tile in shared memory,
-//            link every position to the previous one with the same 15-bit
-//            hash, search every position (F: normal, G: lazy) in parallel,
-//            parse on one thread with a bitmap to skip literal runs, then a
-//            block-wide max-scan marks covered bytes and fills the histogram.
+//   k_lz     one CTA per run of consecutive tiles, sliding the staged window,
+//            the links and the hash table from tile to tile: links built in
+//            parallel chunks plus one ordered table pass, the match and the
+//            lazy match searched at every position in one chain walk (lanes
+//            take new positions as their chains end), the lazy parse split
+//            across lanes with a convergence fix-up, then a block-wide
+//            max-scan marks covered bytes and fills the histogram.
 //   k_huff   one warp per segment: code lengths, canonical codes, block type,
 //            RLE code-length header (deflate_block.cpp:196-290 rules).
 //   k_enc    one warp per tile: resolves tokens 32 positions at a time and
