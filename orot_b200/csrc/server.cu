@@ -503,11 +503,23 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
   // groups: contiguous buffer ranges
   std::vector<size_t> gfirst, gcount;
   std::vector<uint64_t> gsrc, gdst, gcap;
-  uint64_t src = 0, dst = 0;
+  uint64_t src = 0, dst = 0, total = 0;
+  for (size_t i = 0; i < count; ++i) total += in_sizes[i];
+  // Group sizes ramp up (1/8, 1/4, 1/2 of group_bytes) at the start and down
+  // at the end, so that the first kernels start after a short copy and the
+  // last copies out follow a short pass: the pipeline fills and drains fast.
+  const uint64_t G = group_bytes;
   for (size_t i = 0; i < count;) {
+    const uint64_t left = total - src;
+    const size_t gi = gfirst.size();
+    uint64_t target = gi < 3 ? (G >> (3 - gi)) : G;
+    if (left <= G / 8) target = left;
+    else if (left <= 3 * G / 8) target = std::min(target, left - G / 8);
+    else if (left <= 7 * G / 8) target = std::min(target, left - 3 * G / 8);
+    else if (left - target < 7 * G / 8) target = left - 7 * G / 8;
     size_t j = i;
     uint64_t b = 0, ob = 0;
-    while (j < count && (j == i || b + in_sizes[j] <= group_bytes)) {
+    while (j < count && (j == i || b + in_sizes[j] <= target)) {
       b += in_sizes[j];
       ob += align_up(framed_bound(in_sizes[j], int(format)), 16);
       ++j;
