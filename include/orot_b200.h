@@ -90,6 +90,16 @@ size_t deflate_parallel_compress(deflate_parallel_ctx* ctx, const void* in, size
 uint32_t deflate_adler32(uint32_t initial, const void* data, size_t len);
 uint32_t deflate_crc32(uint32_t initial, const void* data, size_t len);
 
+/* Replaces deflate_decompress, include/orot/deflate.h:79-89 (whole buffer,
+ * src/api/deflate_api.cpp:138-219), decoded on the GPU: raw, zlib (header
+ * rules and Adler-32 trailer checked) or gzip (header flags skipped, CRC-32
+ * and ISIZE checked).  Returns DEFLATE_OK with *actual_out_size set;
+ * DEFLATE_DATA_ERROR for corrupt input, truncated input or an output buffer
+ * that is too small (as the reference); DEFLATE_PARAM_ERROR for bad
+ * arguments. */
+deflate_result deflate_decompress(const void* in, size_t in_size, void* out, size_t out_capacity,
+                                  size_t* actual_out_size, deflate_format format);
+
 /* ------------------------------------------------------------------------
  * Extension: device-resident batches (no counterpart in the reference, whose
  * only multi-buffer path is one deflate_compress call per buffer).
@@ -184,6 +194,13 @@ uint64_t deflate_gpu_server_submit(deflate_gpu_server* s, const void* in, size_t
 int deflate_gpu_server_wait(deflate_gpu_server* s, uint64_t ticket, size_t* out_size, double* latency_s,
                             double timeout_s);
 int deflate_gpu_server_stats(deflate_gpu_server* s, uint64_t* passes, uint64_t* max_in_flight);
+
+/* On-device verification of the last run of a batch (no counterpart in the
+ * reference): every stream is decoded on the GPU (one warp per stream),
+ * compared byte for byte with its input, and its framing and trailer are
+ * checked.  ok[i] = 1 for a stream that round-trips.  Returns the number of
+ * streams that failed, or -1. */
+int deflate_gpu_batch_verify(deflate_gpu_batch* b, int* ok);
 
 /* One pigz-style stream compressed by several GPUs (no counterpart in the
  * reference; the unit it shards is the chunk of deflate_parallel_compress,

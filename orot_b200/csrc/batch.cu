@@ -70,6 +70,7 @@ using namespace orotb;
 
 struct deflate_gpu_batch {
   Engine eng;
+  DevBuf d_verify, d_vtab;  // on-device verification: decoded bytes, job tables
   std::vector<Job> jobs;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -233,6 +234,77 @@ int deflate_gpu_batch_sizes(deflate_gpu_batch* b, size_t* out_sizes) {
   }
   for (size_t i = 0; i < s.size(); ++i) out_sizes[i] = s[i].error ? 0 : s[i].out_size;
   return 0;
+}
+
+int deflate_gpu_batch_verify(deflate_gpu_batch* b, int* ok) {
+  if (!b || !b->ran || !ok) return -1;
+  Engine& e = b->eng;
+  if (cudaDeviceSynchronize() != cudaSuccess) { set_error(cudaGetErrorString(cudaGetLastError())); return -1; }
+  const size_t n = e.streams.size();
+  std::vector<Stream> s(n);
+  if (n && cudaMemcpy(s.data(), static_cast<uint8_t*>(e.d_tables.p) + e.off_streams, n * sizeof(Stream),
+                      cudaMemcpyDeviceToHost) != cudaSuccess) {
+    set_error("D2H failed");
+    return -1;
+  }
+  // one decode job per stream (framing stripped), largest streams first
+  std::vector<InflateJob> jobs(n);
+  std::vector<uint64_t> ref_off(n), ref_len(n);
+  std::vector<uint32_t> order;
+  uint64_t vbytes = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const uint32_t hdr = s[i].fmt == kFmtZlib ? 2 : s[i].fmt == kFmtGzip ? 10 : 0;
+    const uint32_t trl = s[i].fmt == kFmtZlib ? 4 : s[i].fmt == kFmtGzip ? 8 : 0;
+    InflateJob& j = jobs[i];
+    ref_off[i] = s[i].in_off;
+    ref_len[i] = s[i].in_len;
+    if (s[i].error || s[i].out_size < hdr + trl + 2) {
+      j.status = kInfData;
+      continue;
+    }
+    j.in_off = s[i].out_off + hdr;
+    j.in_len = s[i].out_size - hdr - trl;
+    j.out_off = vbytes;
+    j.out_cap = s[i].in_len;
+    vbytes += align_up(s[i].in_len, 16);
+    order.push_back(uint32_t(i));
+  }
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return jobs[a].in_len > jobs[c].in_len; });
+  const size_t o_jobs = 0, o_order = align_up(n * sizeof(InflateJob), 256);
+  const size_t o_roff = o_order + align_up(n * 4 + 8, 256), o_rlen = o_roff + align_up(n * 8, 256);
+  const size_t o_cnt = o_rlen + align_up(n * 8, 256);
+  if (!b->d_verify.ensure(vbytes + 256) || !b->d_vtab.ensure(o_cnt + 256)) return -1;
+  uint8_t* vt = static_cast<uint8_t*>(b->d_vtab.p);
+  InflateJob* d_jobs = reinterpret_cast<InflateJob*>(vt + o_jobs);
+  uint32_t* d_order = reinterpret_cast<uint32_t*>(vt + o_order);
+  uint64_t* d_roff = reinterpret_cast<uint64_t*>(vt + o_roff);
+  uint64_t* d_rlen = reinterpret_cast<uint64_t*>(vt + o_rlen);
+  uint32_t* d_cnt = reinterpret_cast<uint32_t*>(vt + o_cnt);
+  cudaStream_t st = e.stream;
+  if ((n && cudaMemcpyAsync(d_jobs, jobs.data(), n * sizeof(InflateJob), cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+      (!order.empty() && cudaMemcpyAsync(d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+      (n && cudaMemcpyAsync(d_roff, ref_off.data(), n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+      (n && cudaMemcpyAsync(d_rlen, ref_len.data(), n * 8, cudaMemcpyHostToDevice, st) != cudaSuccess)) {
+    set_error("H2D failed");
+    return -1;
+  }
+  uint8_t* dec = static_cast<uint8_t*>(b->d_verify.p);
+  launch_inflate(static_cast<const uint8_t*>(e.d_out.p), dec, d_jobs, d_order, uint32_t(order.size()), d_cnt, e.sms, st);
+  launch_inflate_compare(dec, static_cast<const uint8_t*>(e.d_in.p), d_jobs, d_roff, d_rlen, uint32_t(n), st);
+  launch_frame_check(static_cast<const uint8_t*>(e.d_out.p),
+                     reinterpret_cast<const Stream*>(static_cast<uint8_t*>(e.d_tables.p) + e.off_streams), d_jobs,
+                     uint32_t(n), st);
+  if (n && cudaMemcpyAsync(jobs.data(), d_jobs, n * sizeof(InflateJob), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -1;
+  if (cudaStreamSynchronize(st) != cudaSuccess) {
+    set_error(std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
+    return -1;
+  }
+  int bad = 0;
+  for (size_t i = 0; i < n; ++i) {
+    ok[i] = jobs[i].status == kInfOk ? 1 : 0;
+    bad += 1 - ok[i];
+  }
+  return bad;
 }
 
 size_t deflate_gpu_batch_output(deflate_gpu_batch* b, size_t i, void* dst, size_t cap) {

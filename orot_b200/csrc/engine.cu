@@ -404,6 +404,15 @@ uint32_t Engine::checksum_host(uint32_t init, const void* data, size_t n, bool a
   if (n == 0) return init;
   if (!ensure_io(align_up(n, 16), 64) || !h_stage.ensure(n)) return init;
   std::memcpy(h_stage.p, data, n);
+  if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+    set_error("H2D failed");
+    return init;
+  }
+  return checksum_device(init, static_cast<const uint8_t*>(d_in.p), n, adler);
+}
+
+uint32_t Engine::checksum_device(uint32_t init, const uint8_t* d_data, size_t n, bool adler) {
+  if (n == 0) return init;
   // checksum blocks of the whole buffer
   cks.clear();
   for (uint64_t o = 0; o < n; o += 65536) {
@@ -417,12 +426,11 @@ uint32_t Engine::checksum_host(uint32_t init, const void* data, size_t n, bool a
   if (!d_tables.ensure(ck_bytes + 256)) return init;
   uint32_t* d_res = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(d_tables.p) + align_up(ck_bytes, 256));
   Work w{};
-  w.in = static_cast<const uint8_t*>(d_in.p);
+  w.in = d_data;
   w.ck = static_cast<CkBlock*>(d_tables.p);
   w.nck = uint32_t(cks.size());
   uint32_t res = init;
-  if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
-      cudaMemcpyAsync(d_tables.p, cks.data(), ck_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
+  if (cudaMemcpyAsync(d_tables.p, cks.data(), ck_bytes, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
     set_error("H2D failed");
     return init;
   }

@@ -67,6 +67,9 @@ class Engine {
   size_t compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel, size_t block,
                        uint32_t mode = 0, Stream* result = nullptr);
   uint32_t checksum_host(uint32_t init, const void* data, size_t n, bool adler);
+  // Checksum of n bytes already on the device (d_data 16-byte aligned, with
+  // readable padding after the last byte).
+  uint32_t checksum_device(uint32_t init, const uint8_t* d_data, size_t n, bool adler);
   uint32_t pick_tile(uint64_t total_bytes) const;
 
   int device = 0, sms = 148;

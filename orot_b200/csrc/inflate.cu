@@ -1,0 +1,121 @@
+// inflate.cu -- deflate_decompress on the GPU and on-device verification of
+// a compressed batch.
+//
+// deflate_decompress follows the reference's whole-buffer decompress
+// (src/api/deflate_api.cpp:138-219 with src/formats/raw_deflate.cpp:25-55,
+// zlib_wrapper.cpp:104-142, gzip_wrapper.cpp:76-139): the framing is checked
+// on the host, the raw stream is decoded by k_inflate, the trailer is checked
+// against a checksum of the output computed on the device.  Corrupt input, a
+// stream that needs more input and an output buffer that is too small all
+// return DEFLATE_DATA_ERROR, as in the reference.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <vector>
+#include "engine_host.h"
+#include "kernels.cuh"
+#include "../../include/orot_b200.h"
+
+namespace orotb {
+
+// Raw DEFLATE range of a framed stream, checked like the reference's wrappers.
+static deflate_result frame_range(const uint8_t* s, size_t n, int fmt, size_t* off, size_t* len) {
+  if (fmt == int(DEFLATE_FORMAT_RAW)) {
+    *off = 0;
+    *len = n;
+    return DEFLATE_OK;
+  }
+  if (fmt == int(DEFLATE_FORMAT_ZLIB)) {
+    if (n < 6) return DEFLATE_DATA_ERROR;
+    if ((s[0] & 0x0F) != 8) return DEFLATE_DATA_ERROR;                        // CM = 8
+    if (((uint32_t(s[0]) << 8) | s[1]) % 31 != 0) return DEFLATE_DATA_ERROR;  // FCHECK
+    if (s[1] & 0x20) return DEFLATE_DATA_ERROR;                               // no preset dictionary
+    *off = 2;
+    *len = n - 6;
+    return DEFLATE_OK;
+  }
+  if (n < 18 || s[0] != 0x1F || s[1] != 0x8B || s[2] != 8) return DEFLATE_DATA_ERROR;
+  const uint8_t flags = s[3];
+  size_t o = 10;
+  if (flags & 0x04) {  // FEXTRA
+    if (o + 2 > n) return DEFLATE_DATA_ERROR;
+    o += 2 + (size_t(s[o]) | (size_t(s[o + 1]) << 8));
+  }
+  if (flags & 0x08) {  // FNAME
+    while (o < n && s[o] != 0) ++o;
+    ++o;
+  }
+  if (flags & 0x10) {  // FCOMMENT
+    while (o < n && s[o] != 0) ++o;
+    ++o;
+  }
+  if (flags & 0x02) o += 2;  // FHCRC
+  if (o + 8 > n) return DEFLATE_DATA_ERROR;
+  *off = o;
+  *len = n - o - 8;
+  return DEFLATE_OK;
+}
+
+static deflate_result decompress_host(Engine& e, const uint8_t* in, size_t n, uint8_t* out, size_t cap,
+                                      size_t* actual, int fmt) {
+  size_t off = 0, rlen = 0;
+  const deflate_result fr = frame_range(in, n, fmt, &off, &rlen);
+  if (fr != DEFLATE_OK) return fr;
+  if (!e.ensure_io(align_up(rlen, 16) + 64, align_up(cap, 16) + 64)) return DEFLATE_MEM_ERROR;
+  const size_t tbl = align_up(sizeof(InflateJob), 256) + 256;
+  if (!e.d_tables.ensure(tbl) || !e.h_stage.ensure(std::max<size_t>(rlen, sizeof(InflateJob)))) return DEFLATE_MEM_ERROR;
+  uint8_t* dt = static_cast<uint8_t*>(e.d_tables.p);
+  InflateJob* d_job = reinterpret_cast<InflateJob*>(dt);
+  uint32_t* d_order = reinterpret_cast<uint32_t*>(dt + align_up(sizeof(InflateJob), 256));
+  uint32_t* d_counter = d_order + 1;
+  InflateJob job{};
+  job.in_len = rlen;
+  job.out_cap = cap;
+  const uint32_t zero = 0;
+  if (rlen) std::memcpy(e.h_stage.p, in + off, rlen);
+  if ((rlen && cudaMemcpyAsync(e.d_in.p, e.h_stage.p, rlen, cudaMemcpyHostToDevice, e.stream) != cudaSuccess) ||
+      cudaMemcpyAsync(d_job, &job, sizeof job, cudaMemcpyHostToDevice, e.stream) != cudaSuccess ||
+      cudaMemcpyAsync(d_order, &zero, 4, cudaMemcpyHostToDevice, e.stream) != cudaSuccess) {
+    set_error("H2D failed");
+    return DEFLATE_MEM_ERROR;
+  }
+  launch_inflate(static_cast<const uint8_t*>(e.d_in.p), static_cast<uint8_t*>(e.d_out.p), d_job, d_order, 1,
+                 d_counter, e.sms, e.stream);
+  if (cudaMemcpyAsync(&job, d_job, sizeof job, cudaMemcpyDeviceToHost, e.stream) != cudaSuccess ||
+      cudaStreamSynchronize(e.stream) != cudaSuccess) {
+    set_error(std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
+    return DEFLATE_MEM_ERROR;
+  }
+  if (job.status != kInfOk) return DEFLATE_DATA_ERROR;
+  const uint8_t* t = in + n;  // trailer
+  if (fmt == int(DEFLATE_FORMAT_ZLIB)) {
+    const uint32_t want = (uint32_t(t[-4]) << 24) | (uint32_t(t[-3]) << 16) | (uint32_t(t[-2]) << 8) | t[-1];
+    if (e.checksum_device(1, static_cast<const uint8_t*>(e.d_out.p), job.out_len, true) != want) return DEFLATE_DATA_ERROR;
+  } else if (fmt == int(DEFLATE_FORMAT_GZIP)) {
+    const uint32_t crc = uint32_t(t[-8]) | (uint32_t(t[-7]) << 8) | (uint32_t(t[-6]) << 16) | (uint32_t(t[-5]) << 24);
+    const uint32_t isz = uint32_t(t[-4]) | (uint32_t(t[-3]) << 8) | (uint32_t(t[-2]) << 16) | (uint32_t(t[-1]) << 24);
+    if (e.checksum_device(0, static_cast<const uint8_t*>(e.d_out.p), job.out_len, false) != crc) return DEFLATE_DATA_ERROR;
+    if (isz != uint32_t(job.out_len & 0xFFFFFFFFu)) return DEFLATE_DATA_ERROR;
+  }
+  if (job.out_len && cudaMemcpy(out, e.d_out.p, job.out_len, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    set_error("D2H failed");
+    return DEFLATE_MEM_ERROR;
+  }
+  if (actual) *actual = job.out_len;
+  return DEFLATE_OK;
+}
+
+}  // namespace orotb
+
+using namespace orotb;
+
+extern "C" deflate_result deflate_decompress(const void* in, size_t in_size, void* out, size_t out_capacity,
+                                             size_t* actual_out_size, deflate_format format) {
+  const int fmt = int(format);
+  if (fmt < 0 || fmt > 2 || (in_size && !in) || (out_capacity && !out)) return DEFLATE_PARAM_ERROR;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  return decompress_host(global_engine(), static_cast<const uint8_t*>(in), in_size, static_cast<uint8_t*>(out),
+                         out_capacity, actual_out_size, fmt);
+}

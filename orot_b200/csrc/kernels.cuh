@@ -69,4 +69,26 @@ void launch_join(const Work& wk, uint32_t* counter, cudaStream_t st, int sms);
 void launch_frame(const Work& wk, cudaStream_t st);
 void upload_crc_tables();
 
+// One DEFLATE stream to decode (raw data, framing stripped by the host).
+struct InflateJob {
+  uint64_t in_off;   // raw DEFLATE bytes, relative to the input base
+  uint64_t in_len;
+  uint64_t out_off;  // output slot, relative to the output base
+  uint64_t out_cap;
+  uint64_t out_len;  // result: bytes written
+  uint64_t in_used;  // result: bytes of input the stream occupied
+  int32_t status;    // result: kInf*
+  uint32_t pad;
+};
+constexpr int32_t kInfOk = 0, kInfData = 1, kInfOutput = 2, kInfInput = 3, kInfMismatch = 4;
+// Decodes jobs[order[0..n)] (one warp per stream; the input and output
+// buffers carry at least 8 bytes of padding); `counter` is a device word.
+void launch_inflate(const uint8_t* in, uint8_t* out, InflateJob* jobs, const uint32_t* order, uint32_t njobs,
+                    uint32_t* counter, int sms, cudaStream_t st);
+// Marks kInfMismatch on streams whose framing or trailer is wrong (job i is stream i).
+void launch_frame_check(const uint8_t* out, const Stream* streams, InflateJob* jobs, uint32_t n, cudaStream_t st);
+// Marks kInfMismatch on jobs whose decoded bytes differ from ref[ref_off[j], + ref_len[j]).
+void launch_inflate_compare(const uint8_t* decoded, const uint8_t* ref, InflateJob* jobs, const uint64_t* ref_off,
+                            const uint64_t* ref_len, uint32_t njobs, cudaStream_t st);
+
 }  // namespace orotb

@@ -110,6 +110,10 @@ def lib() -> ctypes.CDLL:
                                           c.c_double]
     L.deflate_gpu_server_stats.restype = c.c_int
     L.deflate_gpu_server_stats.argtypes = [c.c_void_p, c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
+    L.deflate_decompress.restype = c.c_int
+    L.deflate_decompress.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.POINTER(c.c_size_t), c.c_int]
+    L.deflate_gpu_batch_verify.restype = c.c_int
+    L.deflate_gpu_batch_verify.argtypes = [c.c_void_p, c.POINTER(c.c_int)]
     L.deflate_gpu_parallel_shard.restype = c.c_int
     L.deflate_gpu_parallel_shard.argtypes = [c.c_void_p, c.c_size_t, c.c_int, c.c_int, c.c_size_t, c.c_int, c.c_void_p,
                                              c.c_size_t, c.POINTER(c.c_size_t), c.POINTER(c.c_uint32)]
@@ -157,6 +161,20 @@ def compress(data, level: int = Level.Default, format: Format = Format.Zlib) -> 
     if r == 0:
         raise Error(DEFLATE_BUF_ERROR, "deflate::compress: output buffer overflow " + last_error())
     return out.raw[:r]
+
+
+def decompress(data, format: Format = Format.Zlib, max_output: int = 256 << 20) -> bytes:
+    """deflate_decompress into a buffer of max_output bytes, decoded on the GPU
+    (include/orot/deflate.h:238-255); raises Error on failure."""
+    L = lib()
+    addr, n, keep = _ptr(data)
+    out = ctypes.create_string_buffer(max(max_output, 1))
+    actual = ctypes.c_size_t(0)
+    r = L.deflate_decompress(addr if n else None, n, out, max_output, ctypes.byref(actual), int(format))
+    del keep
+    if r != DEFLATE_OK:
+        raise Error(r, "deflate::decompress failed " + last_error())
+    return out.raw[:actual.value]
 
 
 class ParallelCompressor:
@@ -343,6 +361,15 @@ class DeviceBatch:
 
     def launches(self) -> int:
         return lib().deflate_gpu_batch_launches(self._b)
+
+    def verify(self) -> list[bool]:
+        """Decodes every stream of the last run on the device and compares it
+        with its input (deflate_gpu_batch_verify); True per stream that
+        round-trips with the right framing and trailer."""
+        ok = (ctypes.c_int * self.count)()
+        if lib().deflate_gpu_batch_verify(self._b, ok) < 0:
+            raise Error(DEFLATE_PARAM_ERROR, "batch verify: " + last_error())
+        return [bool(x) for x in ok]
 
     def profile(self, on: bool) -> None:
         lib().deflate_gpu_batch_profile(self._b, int(on))

@@ -1,0 +1,95 @@
+"""GPU inflate: deflate_decompress (the reference's whole-buffer decompress,
+src/api/deflate_api.cpp:138-219 and src/formats/*) and on-device verification
+of compressed batches.  Streams come from three encoders: this engine, the
+oracle (the reference's encoder restated) and zlib; every decode must equal
+the original bytes, and corrupt, truncated or oversized cases must fail the
+way the reference fails (DEFLATE_DATA_ERROR)."""
+import struct
+import zlib
+
+import pytest
+
+from orot_b200 import deflate, synth
+
+pytestmark = pytest.mark.gpu
+
+DATA_ERROR = -1
+WBITS = {0: -15, 1: 15, 2: 31}
+
+
+def raw_call(blob, fmt, cap):
+    import ctypes
+    L = deflate.lib()
+    out = ctypes.create_string_buffer(max(cap, 1))
+    n = ctypes.c_size_t(0)
+    r = L.deflate_decompress(blob, len(blob), out, cap, ctypes.byref(n), fmt)
+    return r, out.raw[:n.value]
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+@pytest.mark.parametrize("level", [0, 1, 3, 6, 9, 12])
+def test_own_streams_round_trip(gpu, fmt, level):
+    for kind, n in [(synth.MIXED, 3 << 20), (synth.TEXT, 100000), (synth.ZEROS, 70000), (synth.RANDOM, 5000),
+                    (synth.PERIODIC, 1 << 20), (synth.INTS, 0)]:
+        d = synth.gen(n, kind, level + kind)
+        c = deflate.compress(d, level, deflate.Format(fmt))
+        assert deflate.decompress(c, deflate.Format(fmt), n + 16) == d
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+def test_oracle_and_zlib_streams(gpu, oracle, fmt):
+    for kind in range(6):
+        d = synth.gen(400000, kind, 30 + kind)
+        for level in (1, 4, 6, 9):
+            assert deflate.decompress(oracle.compress(d, level, fmt), deflate.Format(fmt), len(d)) == d
+            assert deflate.decompress(oracle.parallel(d, level, fmt, 65536), deflate.Format(fmt), len(d)) == d
+        for zl in (0, 1, 6, 9):
+            c = zlib.compressobj(zl, zlib.DEFLATED, WBITS[fmt])
+            z = c.compress(d) + c.flush()
+            assert deflate.decompress(z, deflate.Format(fmt), len(d)) == d
+
+
+def test_gzip_header_fields(gpu):
+    d = synth.gen(50000, synth.TEXT, 5)
+    c = zlib.compressobj(6, zlib.DEFLATED, -15)
+    body = c.compress(d) + c.flush()
+    extra = b"AB\x04\x00xyzw"
+    hdr = bytes([0x1F, 0x8B, 8, 0x04 | 0x08 | 0x10 | 0x02, 0, 0, 0, 0, 0, 3])
+    hdr += struct.pack("<H", len(extra)) + extra + b"name.txt\x00" + b"a comment\x00"
+    hdr += struct.pack("<H", zlib.crc32(hdr) & 0xFFFF)
+    blob = hdr + body + struct.pack("<II", zlib.crc32(d), len(d))
+    assert deflate.decompress(blob, deflate.Format.Gzip, len(d)) == d
+
+
+def test_errors_like_the_reference(gpu):
+    d = synth.gen(200000, synth.MIXED, 9)
+    for fmt in (1, 2):
+        c = bytearray(deflate.compress(d, 6, deflate.Format(fmt)))
+        r, _ = raw_call(bytes(c), fmt, len(d))
+        assert r == 0
+        bad = bytearray(c)
+        bad[-5 if fmt == 1 else -6] ^= 0x40  # checksum byte
+        assert raw_call(bytes(bad), fmt, len(d))[0] == DATA_ERROR
+        assert raw_call(bytes(c[: len(c) // 2]), fmt, len(d))[0] == DATA_ERROR  # truncated
+        assert raw_call(bytes(c), fmt, len(d) - 1)[0] == DATA_ERROR            # output too small
+    assert raw_call(b"\x78\x9d" + b"\x00" * 10, 1, 100)[0] == DATA_ERROR      # FCHECK
+    assert raw_call(b"\x1f\x8c" + b"\x00" * 20, 2, 100)[0] == DATA_ERROR      # magic
+    assert raw_call(b"\x07\x00\x00", 0, 100)[0] == DATA_ERROR                 # block type 3
+    assert raw_call(b"\x03\x00", 0, 0) == (0, b"")                           # empty fixed block
+    r, out = raw_call(deflate.compress(b"", 6, deflate.Format.Gzip), 2, 0)
+    assert r == 0 and out == b""
+    # exactly full output is fine
+    c = deflate.compress(d, 1, deflate.Format.Raw)
+    assert raw_call(c, 0, len(d)) == (0, d)
+
+
+@pytest.mark.parametrize("level", [1, 6])
+def test_batch_verify_on_device(gpu, level):
+    sizes = [int(x) for x in synth.loguniform_sizes(400, 1, 2 << 20, 3)] + [0, 1, 5]
+    bufs = [synth.gen(n, i % 6, i) for i, n in enumerate(sizes)]
+    for fmt in (deflate.Format.Zlib, deflate.Format.Gzip, deflate.Format.Raw):
+        b = deflate.DeviceBatch()
+        b.load(b"".join(bufs), sizes, level, fmt)
+        b.run()
+        assert all(b.verify())
+        b.close()
