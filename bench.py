@@ -25,6 +25,8 @@ Reported (one JSON line from rank 0):
              latency and sustained GB/s; then the server's capacity (the
              trace submitted at once; mixed, level 1 and level 6) beside the
              plain path.
+  device_verify  every stream of the batch decoded by the GPU inflate and
+             compared with its input on the device (wall time, informational).
 Inputs (5.1 GB) exceed the 126 MB L2, so no flush is needed between steps.
 
 `--impl reference` times the reference's CPU implementation on the same
@@ -404,11 +406,20 @@ def main():
         raise SystemExit("a stream failed to compress")
     comp = sum(out_sizes)
     ratio = comp / total
-    # round-trip check on a sample of the streams
+    # round-trip check on a sample of the streams (zlib on the host) and of
+    # every stream on the device (decoded by the GPU inflate, compared with
+    # its input, framing and trailer checked)
     for i in sample_indices(sizes, 64 << 20, 9)[:200]:
         o = b.output(i, out_sizes[i])
         if zlib.decompress(o) != buf[offs[i]:offs[i + 1]].tobytes():
             raise SystemExit(f"stream {i} does not round-trip")
+    t0 = time.perf_counter()
+    vok = b.verify()
+    verify_s = time.perf_counter() - t0
+    if not all(vok):
+        raise SystemExit(f"{len(vok) - sum(vok)} streams fail the on-device round trip")
+    device_verify = {"streams": len(vok), "ok": int(sum(vok)), "wall_ms": verify_s * 1e3,
+                     "inflate_GBps_wall": total / verify_s / 1e9}
 
     # -- per-phase times (profiled passes, events between phases)
     b.profile(True)
@@ -506,6 +517,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "ratio": ratio, "gpu_launches": launches_per_pass * args.steps, "e2e": e2e, "plain": plain,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
+            "device_verify": device_verify,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -30,6 +30,8 @@ namespace {
 constexpr uint32_t kAll = 0xFFFFFFFFu;
 constexpr int kFastBits = 9;
 constexpr uint32_t kFast = 1u << kFastBits;
+constexpr uint32_t kWin = 8192;   // recent output kept in shared memory per warp
+constexpr int kInfWarps = 4;      // warps per CTA
 
 // RFC 1951 3.2.5: base lengths / distances and extra bits of symbols 257..285
 // and distance codes 0..29.
@@ -50,7 +52,9 @@ struct Code {
   uint16_t* sym;    // [nsym]
 };
 
-// Per-warp shared memory.
+// Per-warp shared memory.  Output goes to global memory and to `win`: a match
+// whose source lies in the window reads shared memory instead of waiting for
+// the bytes this warp has just stored to come back from L2.
 struct WarpMem {
   uint16_t lfast[kFast], dfast[kFast];
   uint16_t lcount[16], dcount[16];
@@ -58,6 +62,7 @@ struct WarpMem {
   uint16_t first[16], offs[16];  // builder scratch: first code and first index per length
   uint8_t lens[320];
   uint32_t bad;                  // builder result
+  uint8_t win[kWin];             // the last kWin output bytes, at position & (kWin - 1)
 };
 
 // Builds `c` from code lengths lens[0..n) (all lanes).  Returns false for an
@@ -158,10 +163,10 @@ __device__ __forceinline__ uint32_t decode(BitIn& b, const Code& c) {
 }  // namespace
 
 // status: kInfOk, kInfData (corrupt), kInfOutput (output full), kInfInput (input exhausted)
-__global__ void __launch_bounds__(256) k_inflate(const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
+__global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
                                                  InflateJob* jobs, const uint32_t* __restrict__ order, uint32_t njobs,
                                                  uint32_t* counter) {
-  __shared__ WarpMem wm[8];
+  __shared__ WarpMem wm[kInfWarps];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   WarpMem& m = wm[wid];
   const Code lit{m.lfast, m.lcount, m.lsym}, dst{m.dfast, m.dcount, m.dsym};
@@ -210,7 +215,11 @@ __global__ void __launch_bounds__(256) k_inflate(const uint8_t* __restrict__ in,
         if (src + len > job.in_len) { status = kInfInput; break; }
         if (op + len > job.out_cap) { status = kInfOutput; break; }
         const uint8_t* s = in + job.in_off + src;
-        for (uint32_t i = lane; i < len; i += 32) o[op + i] = s[i];
+        for (uint32_t i = lane; i < len; i += 32) {
+          const uint8_t v = s[i];
+          o[op + i] = v;
+          m.win[(op + i) & (kWin - 1)] = v;
+        }
         op += len;
         __syncwarp();
         continue;
@@ -290,7 +299,9 @@ __global__ void __launch_bounds__(256) k_inflate(const uint8_t* __restrict__ in,
             const uint32_t sym = decode(b, lit);
             if (sym < 256) {
               if (op >= job.out_cap) { st = kInfOutput; cmd = 2; break; }
-              o[op++] = uint8_t(sym);
+              o[op] = uint8_t(sym);
+              m.win[op & (kWin - 1)] = uint8_t(sym);
+              ++op;
               continue;
             }
             if (sym == 256) { cmd = 0; break; }
@@ -317,7 +328,15 @@ __global__ void __launch_bounds__(256) k_inflate(const uint8_t* __restrict__ in,
         dist = __shfl_sync(kAll, dist, 0);
         const uint64_t p0 = __shfl_sync(kAll, op, 0);
         __syncwarp();
-        for (uint32_t i = lane; i < len; i += 32) o[p0 + i] = o[p0 - dist + (i % dist)];
+        // sources lie before p0; in the window unless the copy's own writes
+        // could reach the slots other lanes read (dist + len > kWin)
+        const bool in_win = dist + len <= kWin;
+        for (uint32_t i = lane; i < len; i += 32) {
+          const uint64_t src = p0 - dist + (i < dist ? i : i % dist);
+          const uint8_t v = in_win ? m.win[src & (kWin - 1)] : o[src];
+          o[p0 + i] = v;
+          m.win[(p0 + i) & (kWin - 1)] = v;
+        }
         __syncwarp();
         if (lane == 0) op += len;
       }
@@ -383,10 +402,10 @@ void launch_inflate(const uint8_t* in, uint8_t* out, InflateJob* jobs, const uin
                     uint32_t* counter, int sms, cudaStream_t st) {
   if (!njobs) return;
   cudaMemsetAsync(counter, 0, 4, st);
-  uint32_t blocks = uint32_t(sms) * 4;  // 8 warps each; 32 warps per SM
-  const uint32_t need = (njobs + 7) / 8;
+  uint32_t blocks = uint32_t(sms) * 4;  // 4 CTAs of 4 warps per SM (shared memory)
+  const uint32_t need = (njobs + kInfWarps - 1) / kInfWarps;
   if (blocks > need) blocks = need;
-  k_inflate<<<blocks, 256, 0, st>>>(in, out, jobs, order, njobs, counter);
+  k_inflate<<<blocks, kInfWarps * 32, 0, st>>>(in, out, jobs, order, njobs, counter);
 }
 
 void launch_inflate_compare(const uint8_t* decoded, const uint8_t* ref, InflateJob* jobs, const uint64_t* ref_off,
