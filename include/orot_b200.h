@@ -195,6 +195,18 @@ int deflate_gpu_server_wait(deflate_gpu_server* s, uint64_t ticket, size_t* out_
                             double timeout_s);
 int deflate_gpu_server_stats(deflate_gpu_server* s, uint64_t* passes, uint64_t* max_in_flight);
 
+/* gzip files of independent members (no counterpart in the reference's
+ * compress API; the form pigz --independent writes): the input is cut into
+ * members of member_size bytes, each a complete gzip stream at `level`, all
+ * compressed in one pass.  Every gzip reader reads the concatenation as one
+ * file; deflate_decompress decodes its members in parallel (the reference's
+ * parallel gzip path, src/decompress/parallel_decompress.cpp:64-150).  Returns
+ * the byte count, or 0 when out_capacity is below
+ * deflate_gzip_members_bound() or on a device error. */
+size_t deflate_gzip_members_bound(size_t in_size, size_t member_size);
+size_t deflate_gpu_compress_gzip_members(const void* in, size_t in_size, int level, size_t member_size, void* out,
+                                         size_t out_capacity);
+
 /* On-device verification of the last run of a batch (no counterpart in the
  * reference): every stream is decoded on the GPU (one warp per stream),
  * compared byte for byte with its input, and its framing and trailer are

@@ -58,8 +58,17 @@ static deflate_result frame_range(const uint8_t* s, size_t n, int fmt, size_t* o
   return DEFLATE_OK;
 }
 
+deflate_result gzip_members_decompress(Engine& e, const uint8_t* in, size_t n, uint8_t* out, size_t cap,
+                                       size_t* actual);
+
 static deflate_result decompress_host(Engine& e, const uint8_t* in, size_t n, uint8_t* out, size_t cap,
                                       size_t* actual, int fmt) {
+  // gzip of 256 KiB or more: independent members decode in parallel when there
+  // are at least two (src/api/deflate_api.cpp:203-211); otherwise one stream
+  if (fmt == int(DEFLATE_FORMAT_GZIP) && n >= (size_t(256) << 10)) {
+    const deflate_result r = gzip_members_decompress(e, in, n, out, cap, actual);
+    if (r != DEFLATE_DATA_ERROR) return r;
+  }
   size_t off = 0, rlen = 0;
   const deflate_result fr = frame_range(in, n, fmt, &off, &rlen);
   if (fr != DEFLATE_OK) return fr;

@@ -112,6 +112,10 @@ def lib() -> ctypes.CDLL:
     L.deflate_gpu_server_stats.argtypes = [c.c_void_p, c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     L.deflate_decompress.restype = c.c_int
     L.deflate_decompress.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.POINTER(c.c_size_t), c.c_int]
+    L.deflate_gzip_members_bound.restype = c.c_size_t
+    L.deflate_gzip_members_bound.argtypes = [c.c_size_t, c.c_size_t]
+    L.deflate_gpu_compress_gzip_members.restype = c.c_size_t
+    L.deflate_gpu_compress_gzip_members.argtypes = [c.c_void_p, c.c_size_t, c.c_int, c.c_size_t, c.c_void_p, c.c_size_t]
     L.deflate_gpu_batch_verify.restype = c.c_int
     L.deflate_gpu_batch_verify.argtypes = [c.c_void_p, c.POINTER(c.c_int)]
     L.deflate_gpu_parallel_shard.restype = c.c_int
@@ -175,6 +179,20 @@ def decompress(data, format: Format = Format.Zlib, max_output: int = 256 << 20) 
     if r != DEFLATE_OK:
         raise Error(r, "deflate::decompress failed " + last_error())
     return out.raw[:actual.value]
+
+
+def compress_gzip_members(data, level: int = Level.Default, member_size: int = 1 << 20) -> bytes:
+    """One gzip file of independent members of member_size input bytes
+    (deflate_gpu_compress_gzip_members)."""
+    L = lib()
+    addr, n, keep = _ptr(data)
+    cap = L.deflate_gzip_members_bound(n, member_size)
+    out = ctypes.create_string_buffer(max(cap, 1))
+    r = L.deflate_gpu_compress_gzip_members(addr if n else None, n, int(level), member_size, out, cap)
+    del keep
+    if r == 0:
+        raise Error(DEFLATE_BUF_ERROR, "compress_gzip_members failed " + last_error())
+    return out.raw[:r]
 
 
 class ParallelCompressor:

@@ -93,3 +93,35 @@ def test_batch_verify_on_device(gpu, level):
         b.run()
         assert all(b.verify())
         b.close()
+
+
+@pytest.mark.parametrize("level", [1, 6, 9])
+def test_gzip_members_compress_and_parallel_decode(gpu, oracle, level):
+    """Independent members: any gzip reader (zlib with concatenated members)
+    reads the whole file, every member is a complete gzip stream, and
+    deflate_decompress decodes members in parallel (inputs >= 256 KiB)."""
+    d = synth.array((6 << 20) + 777, synth.MIXED, level)
+    blob = deflate.compress_gzip_members(d, level, 1 << 20)
+    # zlib reads concatenated members one at a time
+    out, rest, pos = b"", blob, 0
+    while rest:
+        dobj = zlib.decompressobj(31)
+        out += dobj.decompress(rest)
+        rest = dobj.unused_data
+        pos += 1
+    assert out == d.tobytes() and pos == 7
+    assert deflate.decompress(blob, deflate.Format.Gzip, len(d)) == d.tobytes()
+    # members of the reference's encoder decode the same way
+    ref = b"".join(oracle.compress(d[i:i + (1 << 20)].tobytes(), level, 2) for i in range(0, len(d), 1 << 20))
+    assert deflate.decompress(ref, deflate.Format.Gzip, len(d)) == d.tobytes()
+
+
+def test_gzip_members_errors(gpu):
+    d = synth.array(3 << 20, synth.TEXT, 4)
+    blob = bytearray(deflate.compress_gzip_members(d, 6, 1 << 20))
+    # output smaller than the members' total: MEM_ERROR, as the reference's parallel path
+    assert raw_call(bytes(blob), 2, len(d) - 1)[0] == -2
+    # a damaged member CRC fails the parallel path, and the one-stream fallback fails too
+    first_end = len(deflate.compress_gzip_members(d[: 1 << 20], 6, 1 << 20))
+    blob[first_end - 8] ^= 1
+    assert raw_call(bytes(blob), 2, len(d))[0] == DATA_ERROR
