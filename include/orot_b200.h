@@ -90,6 +90,29 @@ size_t deflate_parallel_compress(deflate_parallel_ctx* ctx, const void* in, size
 uint32_t deflate_adler32(uint32_t initial, const void* data, size_t len);
 uint32_t deflate_crc32(uint32_t initial, const void* data, size_t len);
 
+/* deflate_flush -- include/orot/deflate.h:42-47 (same values) */
+typedef enum deflate_flush {
+  DEFLATE_NO_FLUSH = 0,
+  DEFLATE_SYNC_FLUSH = 1,
+  DEFLATE_FULL_FLUSH = 2,
+  DEFLATE_FINISH = 3
+} deflate_flush;
+
+/* Replaces the streaming compressor, include/orot/deflate.h:92-108
+ * (src/api/stream_api.cpp:134-247).  Input is compressed on the GPU in 1 MiB
+ * chunks, each an independent part of the stream that ends on a byte
+ * boundary; SYNC and FULL flush compress the partial chunk (all input so far
+ * becomes decodable), FINISH writes the last part and the zlib / gzip trailer
+ * and then returns DEFLATE_STREAM_END.  Returns DEFLATE_OK when the input is
+ * consumed and no output is pending, DEFLATE_NEED_OUTPUT when *avail_out ran
+ * out first (call again with more room), DEFLATE_PARAM_ERROR for bad
+ * arguments or input after the end, DEFLATE_MEM_ERROR on a device failure. */
+typedef struct deflate_stream deflate_stream;
+deflate_stream* deflate_stream_new(int level, deflate_format format);
+void deflate_stream_free(deflate_stream* s);
+deflate_result deflate_stream_compress(deflate_stream* s, const uint8_t** next_in, size_t* avail_in,
+                                       uint8_t** next_out, size_t* avail_out, deflate_flush flush);
+
 /* Replaces deflate_decompress, include/orot/deflate.h:79-89 (whole buffer,
  * src/api/deflate_api.cpp:138-219), decoded on the GPU: raw, zlib (header
  * rules and Adler-32 trailer checked) or gzip (header flags skipped, CRC-32

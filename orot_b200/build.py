@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels_fast.cu", "kernels_lazy.cu", "kernels_common.cu", "engine.cu", "batch.cu", "server.cu",
               "shard.cu", "kernels_inflate.cu", "inflate.cu",
-              "members.cu"]
+              "members.cu", "stream.cu"]
 LIB = os.path.join(HERE, "liborot_b200.so")
 SYNTH = os.path.join(HERE, "libsynth.so")
 

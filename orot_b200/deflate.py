@@ -112,6 +112,12 @@ def lib() -> ctypes.CDLL:
     L.deflate_gpu_server_stats.argtypes = [c.c_void_p, c.POINTER(c.c_uint64), c.POINTER(c.c_uint64)]
     L.deflate_decompress.restype = c.c_int
     L.deflate_decompress.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.POINTER(c.c_size_t), c.c_int]
+    L.deflate_stream_new.restype = c.c_void_p
+    L.deflate_stream_new.argtypes = [c.c_int, c.c_int]
+    L.deflate_stream_free.argtypes = [c.c_void_p]
+    L.deflate_stream_compress.restype = c.c_int
+    L.deflate_stream_compress.argtypes = [c.c_void_p, c.POINTER(c.c_void_p), c.POINTER(c.c_size_t),
+                                          c.POINTER(c.c_void_p), c.POINTER(c.c_size_t), c.c_int]
     L.deflate_gzip_members_bound.restype = c.c_size_t
     L.deflate_gzip_members_bound.argtypes = [c.c_size_t, c.c_size_t]
     L.deflate_gpu_compress_gzip_members.restype = c.c_size_t
@@ -193,6 +199,62 @@ def compress_gzip_members(data, level: int = Level.Default, member_size: int = 1
     if r == 0:
         raise Error(DEFLATE_BUF_ERROR, "compress_gzip_members failed " + last_error())
     return out.raw[:r]
+
+
+NO_FLUSH, SYNC_FLUSH, FULL_FLUSH, FINISH = 0, 1, 2, 3
+DEFLATE_STREAM_END, DEFLATE_NEED_OUTPUT = 1, 3
+
+
+class Compressor:
+    """Streaming compressor over deflate_stream_* (the reference's RAII
+    Compressor, include/orot/deflate.h:260-301): feed() takes input and returns
+    whatever compressed bytes are ready, flush() and finish() force output."""
+
+    def __init__(self, level: int = Level.Default, fmt: Format = Format.Zlib):
+        self._s = lib().deflate_stream_new(int(level), int(fmt))
+        if not self._s:
+            raise Error(DEFLATE_MEM_ERROR, "Compressor: allocation failed")
+
+    def _run(self, data, mode: int) -> bytes:
+        L = lib()
+        addr, n, keep = _ptr(data) if data is not None and len(data) else (0, 0, None)
+        nin = ctypes.c_void_p(addr or None)
+        ain = ctypes.c_size_t(n)
+        chunks = []
+        while True:
+            cap = 1 << 20
+            buf = ctypes.create_string_buffer(cap)
+            nout = ctypes.c_void_p(ctypes.addressof(buf))
+            aout = ctypes.c_size_t(cap)
+            r = L.deflate_stream_compress(self._s, ctypes.byref(nin), ctypes.byref(ain), ctypes.byref(nout),
+                                          ctypes.byref(aout), mode)
+            if r < 0:
+                raise Error(r, "Compressor failed " + last_error())
+            chunks.append(buf.raw[:cap - aout.value])
+            if r == DEFLATE_NEED_OUTPUT or (r == DEFLATE_OK and ain.value):
+                continue
+            del keep
+            return b"".join(chunks)
+
+    def feed(self, data) -> bytes:
+        return self._run(data, NO_FLUSH)
+
+    def flush(self, full: bool = False) -> bytes:
+        return self._run(None, FULL_FLUSH if full else SYNC_FLUSH)
+
+    def finish(self) -> bytes:
+        return self._run(None, FINISH)
+
+    def close(self) -> None:
+        if self._s:
+            lib().deflate_stream_free(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class ParallelCompressor:
