@@ -6,10 +6,13 @@
 // same 16-bit hash, newest first; up to max_chain members examined, a 4-byte
 // mismatch counts as a miss and miss_limit consecutive misses end the walk,
 // the longest match wins (ties keep the nearest), nice_len ends the walk;
-// the lazy step searches pos+1 with half the chain and needs two more bytes.
+// the lazy step moves to pos+1 when the match there is two bytes longer.
 // GPU-native differences, all keeping the stream valid:
 //   * a chain ends at the 32 KiB window edge (the reference keeps walking
 //     with distances taken mod 32768);
+//   * every position is searched once with the full chain, and the lazy
+//     step uses that match (the reference searches pos+1 again with half the
+//     chain, skipping the candidate at distance 1);
 //   * the input is cut into independent 4 KiB tiles (16 x 258 bytes): each
 //     tile parses from its own first byte and matches do not run past its
 //     end, while still referencing up to 32 KiB before the tile;
@@ -21,9 +24,9 @@
 //
 //   k_lz     one CTA per run of consecutive tiles, sliding the staged window,
 //            the links and the hash table from tile to tile: links built in
-//            parallel chunks plus one ordered table pass, the match and the
-//            lazy match searched at every position in one chain walk (lanes
-//            take new positions as their chains end), the lazy parse split
+//            parallel chunks plus one ordered table pass, the match searched
+//            at every position (lanes take new positions as their chains
+//            end), the lazy parse split
 //            across lanes with a convergence fix-up, then a block-wide
 //            max-scan marks covered bytes and fills the histogram.
 //   k_huff   one warp per segment: code lengths, canonical codes, block type,
@@ -46,15 +49,15 @@ constexpr uint32_t kRegion = W + T;                            // positions with
 constexpr uint32_t kDataBytes = (W + T + 48 + 127) / 128 * 128;  // + align + over-read tail
 constexpr uint32_t kLinkBytes = (kRegion * 2 + 127) / 128 * 128;  // u16 per position
 constexpr uint32_t kTblBytes = 65536;                          // u16 per 15-bit hash, kept across a run
-constexpr uint32_t kFgBytes = T * 8;                           // F[T] + G[T]; link marks before the search
+constexpr uint32_t kFBytes = T * 4;                            // F[T]; link marks before the search
 constexpr uint32_t kTokBytes = T * 4;
 constexpr uint32_t kFmWords = T / 32;
-constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFgBytes + kTokBytes + kFmWords * 4 + 320 * 4 +
+constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFBytes + kTokBytes + kFmWords * 4 + 320 * 4 +
                              64 * 4;
 static_assert(T % 32 == 0, "tiles are whole windows of 32 positions");
 static_assert(kSmemLz <= 227 * 1024, "one CTA per SM");
 static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words of links");
-static_assert((kRegion + 31) / 32 * 8 <= kFgBytes, "first/last marks of every link chunk fit F");
+static_assert((kRegion + 31) / 32 * 8 <= kFBytes, "first/last marks of every link chunk fit F");
 
 constexpr uint32_t kSerialParse = 128;  // at most this many match positions: serial parse
 
@@ -81,77 +84,50 @@ struct SmemBytes {
 __device__ __forceinline__ uint32_t hash16(uint32_t v) { return (v * 0x9E3779B1u) >> 16; }
 __device__ __forceinline__ uint32_t hash15(uint32_t v) { return (v * 0x9E3779B1u) >> 17; }
 
-// The match at r (every candidate, `chain` steps) and the lazy match at r
-// (candidate r - 1 excluded, `gchain` steps) in one walk of the chain: both
-// searches visit the same candidates in the same order, so each follows the
-// single-search rules exactly (hash-16 filter, step and miss limits, the
-// quick reject, early exit at nice or the longest possible length) while the
-// loads and byte comparisons are shared.  The walk advances one candidate per
-// lz_step call so that a lane can start its next position as soon as its
-// chain ends.
+// The longest match at region position r, walking the chain newest first
+// with the reference's rules (src/deflate/lz77.cpp:66-156): candidates of the
+// same 15-bit bucket but another 16-bit hash are skipped, `chain` candidates
+// with the same 16-bit hash are examined, miss_limit consecutive 4-byte
+// mismatches end the walk, the quick reject at byte `best` skips candidates
+// that cannot be longer, ties keep the nearest, nice length ends the walk.
+// The walk advances one candidate per lz_step call so that a lane can start
+// its next position as soon as its chain ends.
 struct LzState {
-  uint32_t r, v4p, h16p, q, maxm;
-  uint32_t bestF, bdF, bestG, bdG;
-  int stepsF, missF, budF, stepsG, missG, budG;
-  bool onF, onG;
+  uint32_t r, v4p, h16p, q, maxm, best, bd;
+  int steps, miss, bud;
 };
 
-__device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, uint32_t r, uint32_t maxm, int chain,
-                                         int gchain) {
+__device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, uint32_t r, uint32_t maxm, int chain) {
   s.r = r;
   s.q = r;
   s.v4p = sd.load4(r);
   s.h16p = hash16(s.v4p);
   s.maxm = maxm;
-  s.bestF = s.bestG = 2;
-  s.bdF = s.bdG = 0;
-  s.stepsF = chain;
-  s.budF = 2 * chain + 64;
-  s.stepsG = gchain;
-  s.budG = 2 * gchain + 64;
-  s.missF = s.missG = 0;
-  s.onF = true;
-  s.onG = gchain > 0;
+  s.best = 2;
+  s.bd = 0;
+  s.steps = chain;
+  s.miss = 0;
+  s.bud = 2 * chain + 64;  // bounds the filtered candidates too
 }
 
-// One candidate; returns true once both searches have ended.
+// One candidate; returns true once the search has ended.
 __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const uint16_t* __restrict__ link, int nice,
                                         int miss_limit) {
-  if (s.onF && s.budF-- <= 0) s.onF = false;
-  if (s.onG && s.budG-- <= 0) s.onG = false;
-  if (!s.onF && !s.onG) return true;
+  if (s.bud-- <= 0) return true;
   const uint32_t l = link[s.q];
   if (!l) return true;
   s.q -= l;
   const uint32_t q = s.q, r = s.r;
   if (r - q > 32767u) return true;
-  bool useF = s.onF, useG = s.onG && q != r - 1;
-  if (!useF && !useG) return false;
   const uint32_t v = sd.load4(q);
   if (v != s.v4p && hash16(v) != s.h16p) return false;  // same 15-bit bucket, other 16-bit chain
-  if (useF) {
-    if (s.stepsF == 0) s.onF = useF = false;
-    else --s.stepsF;
-  }
-  if (useG) {
-    if (s.stepsG == 0) s.onG = useG = false;
-    else --s.stepsG;
-  }
-  if (v != s.v4p) {
-    if (useF && ++s.missF >= miss_limit) s.onF = false;
-    if (useG && ++s.missG >= miss_limit) s.onG = false;
-    return false;
-  }
-  if (useF) s.missF = 0;
-  if (useG) s.missG = 0;
-  // quick reject (src/deflate/lz77.cpp:137-142): a search improves only on
-  // a candidate whose first best + 1 bytes all match, so 4 bytes ending at
-  // the smaller best of the searches still open decide for both; a
-  // candidate let through here is measured and cannot change a result
-  const uint32_t maxm = s.maxm;
-  const uint32_t mb = min(useF ? s.bestF : 0xFFFFu, useG ? s.bestG : 0xFFFFu);
+  if (s.steps-- == 0) return true;
+  if (v != s.v4p) return ++s.miss >= miss_limit;
+  s.miss = 0;
+  // quick reject (src/deflate/lz77.cpp:137-142), on the 4 bytes ending at
+  // byte `best`: a longer match needs all of them
+  const uint32_t maxm = s.maxm, mb = s.best;
   if (mb >= 4 && mb < maxm && sd.load4(q + mb - 3) != sd.load4(r + mb - 3)) return false;
-  const bool needF = useF, needG = useG;
   uint32_t len = 4;
   while (len < maxm) {
     const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
@@ -159,16 +135,10 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
     len += 4;
   }
   if (len > maxm) len = maxm;
-  const bool stop = int(len) >= nice || len >= maxm;
-  if (needF && len > s.bestF) {
-    s.bestF = len;
-    s.bdF = r - q;
-    if (stop) s.onF = false;
-  }
-  if (needG && len > s.bestG) {
-    s.bestG = len;
-    s.bdG = r - q;
-    if (stop) s.onG = false;
+  if (len > s.best) {
+    s.best = len;
+    s.bd = r - q;
+    if (int(len) >= nice || len >= maxm) return true;
   }
   return false;
 }
@@ -183,13 +153,15 @@ __device__ __forceinline__ uint32_t next_head(const uint32_t* fm, uint32_t i, ui
 }
 
 // One step of the lazy parse from head i (F[i] != 0): up to `lazy` moves to
-// i + 1 while the lazy match there is longer by two or more.  Returns
+// i + 1 while the match there is longer by two or more (the reference's lazy
+// rule, lz77.cpp:449-493; the match at i + 1 is the full search of i + 1,
+// where the reference searches again with half the chain).  Returns
 // {match position, len << 16 | dist}.
-__device__ __forceinline__ uint2 lazy_step(const uint32_t* F, const uint32_t* G, uint32_t i, uint32_t tl, int lazy) {
+__device__ __forceinline__ uint2 lazy_step(const uint32_t* F, uint32_t i, uint32_t tl, int lazy) {
   uint32_t m = F[i];
   int k = lazy;
   while (k > 0 && i + (m >> 16) + 1 < tl && i + 4 <= tl) {
-    const uint32_t g = G[i + 1];
+    const uint32_t g = F[i + 1];
     if ((g >> 16) > (m >> 16) + 1) {
       ++i;
       m = g;
@@ -260,8 +232,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
   uint16_t* tbl = reinterpret_cast<uint16_t*>(sm + kDataBytes + kLinkBytes);
   uint8_t* fgb = sm + kDataBytes + kLinkBytes + kTblBytes;
   uint32_t* F = reinterpret_cast<uint32_t*>(fgb);
-  uint32_t* G = F + T;
-  uint32_t* tok_s = reinterpret_cast<uint32_t*>(fgb + kFgBytes);
+  uint32_t* tok_s = reinterpret_cast<uint32_t*>(fgb + kFBytes);
   uint32_t* fm = tok_s + T;
   uint32_t* hist = fm + kFmWords;
   uint32_t* scan = hist + 320;
@@ -272,7 +243,6 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
   const uint32_t last = first + runs[2 * blockIdx.x + 1];
   const Segment sg = wk.segs[wk.tiles[first].seg];
   const LazyCfg cfg = c_lazy[sg.level];
-  const uint32_t lazy_chain = cfg.chain > 1 ? uint32_t(cfg.chain) >> 1 : 1u;
   uint32_t prev_rs = 0, prev_nreg = 0;
 
   for (uint32_t ti = first; ti < last; ++ti) {
@@ -336,7 +306,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     // read and one table write per distinct hash.
     {
       const uint32_t nch = (nreg - lstart + 31) / 32;
-      uint32_t* fbits = F;  // F/G are free until the searches
+      uint32_t* fbits = F;  // F is free until the searches
       uint32_t* lbits = F + nch;
       const uint32_t lt = (1u << lane) - 1;
       for (uint32_t c = wid; c < nch; c += blockDim.x >> 5) {
@@ -393,9 +363,8 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     {
       const uint32_t nsearch = tl >= 4 ? tl - 3 : 0;
       const uint32_t nch = (nsearch + 31) / 32;
-      for (uint32_t i = nsearch + tid; i < kFmWords * 32; i += blockDim.x) F[i] = G[i] = 0;
+      for (uint32_t i = nsearch + tid; i < kFmWords * 32; i += blockDim.x) F[i] = 0;
       const uint32_t lt = (1u << lane) - 1;
-      const int gchain = cfg.lazy ? int(lazy_chain) : 0;
       uint32_t pool = 0, avail = 0;  // warp-uniform: next position of the chunk, positions left
       bool more = true;
       uint32_t i = kAll;             // this lane's position
@@ -417,7 +386,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
           const uint32_t take = min(uint32_t(__popc(idle)), avail);
           if (i == kAll && __popc(idle & lt) < take) {
             i = pool + __popc(idle & lt);
-            lz_begin(st, sd, ts - rs + i, min(258u, tl - i), cfg.chain, gchain);
+            lz_begin(st, sd, ts - rs + i, min(258u, tl - i), cfg.chain);
           }
           pool += take;
           avail -= take;
@@ -425,8 +394,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
         }
         if (idle == kAll) break;
         if (i != kAll && lz_step(st, sd, link, cfg.nice, cfg.miss)) {
-          F[i] = st.bestF >= 3 ? (st.bestF << 16) | st.bdF : 0u;
-          G[i] = st.bestG >= 3 ? (st.bestG << 16) | st.bdG : 0u;
+          F[i] = st.best >= 3 ? (st.best << 16) | st.bd : 0u;
           i = kAll;
         }
       }
@@ -459,7 +427,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
           uint32_t i = 0;
           while ((i = next_head(fm, i, tl)) < tl) {
             hd[i >> 5] |= 1u << (i & 31);
-            const uint2 m = lazy_step(F, G, i, tl, cfg.lazy);
+            const uint2 m = lazy_step(F, i, tl, cfg.lazy);
             i = (m.x & 0xFFFFu) + (m.y >> 16);
           }
         }
@@ -470,7 +438,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
           i = next_head(fm, i, tl);
           if (i >= b) break;
           atomicOr(&hd[i >> 5], 1u << (i & 31));
-          const uint2 m = lazy_step(F, G, i, tl, cfg.lazy);
+          const uint2 m = lazy_step(F, i, tl, cfg.lazy);
           i = (m.x & 0xFFFFu) + (m.y >> 16);
         }
         sx[lane] = i;
@@ -494,7 +462,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
                 break;
               }
               hd[h >> 5] |= 1u << (h & 31);
-              const uint2 m = lazy_step(F, G, h, tl, cfg.lazy);
+              const uint2 m = lazy_step(F, h, tl, cfg.lazy);
               i2 = (m.x & 0xFFFFu) + (m.y >> 16);
               clear_bits(hd, h + 1, min(i2, b2));
               if (i2 >= b2) {
@@ -508,7 +476,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
       __syncthreads();
       for (uint32_t i = tid; i < tl; i += blockDim.x) {
         if ((hd[i >> 5] >> (i & 31)) & 1u) {
-          const uint2 m = lazy_step(F, G, i, tl, cfg.lazy);
+          const uint2 m = lazy_step(F, i, tl, cfg.lazy);
           tok_s[m.x & 0xFFFFu] = 0x80000000u | m.y;
         }
       }
