@@ -16,8 +16,11 @@
 //   * the input is cut into independent 4 KiB tiles (16 x 258 bytes): each
 //     tile parses from its own first byte and matches do not run past its
 //     end, while still referencing up to 32 KiB before the tile;
-//   * levels 10-12 use the same chains with 1024/2048/4096 steps and lazy
-//     depth 3 instead of the reference's binary tree;
+//   * levels 10-12 use the same chains with 1024/2048/4096 steps instead of
+//     the reference's binary tree, and an optimal parse: costs from the
+//     histogram of a lazy parse, then a backward pass over the tile picks the
+//     cheapest literal / match (the found match shortened by up to 31 bytes)
+//     at every position;
 //   * code lengths come from an optimal two-queue Huffman construction with
 //     the ITU-T T.81 Annex K.3 length limiter, and the block type is chosen
 //     on exact sizes (the reference uses a flat header estimate).
@@ -52,8 +55,9 @@ constexpr uint32_t kTblBytes = 65536;                          // u16 per 15-bit
 constexpr uint32_t kFBytes = T * 4;                            // F[T]; link marks before the search
 constexpr uint32_t kTokBytes = T * 4;
 constexpr uint32_t kFmWords = T / 32;
+constexpr uint32_t kOptBytes = T * 2 + 320 * 2 + 260 * 2;      // optimal parse: choice[T], symbol and length costs
 constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFBytes + kTokBytes + kFmWords * 4 + 320 * 4 +
-                             64 * 4;
+                             64 * 4 + kOptBytes;
 static_assert(T % 32 == 0, "tiles are whole windows of 32 positions");
 static_assert(kSmemLz <= 227 * 1024, "one CTA per SM");
 static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words of links");
@@ -61,12 +65,13 @@ static_assert((kRegion + 31) / 32 * 8 <= kFBytes, "first/last marks of every lin
 
 constexpr uint32_t kSerialParse = 128;  // at most this many match positions: serial parse
 
-struct LazyCfg { int chain, nice, lazy, miss; };
+// chain, nice, lazy depth, miss limit, optimal parse (levels 10-12)
+struct LazyCfg { int chain, nice, lazy, miss, opt; };
 __constant__ LazyCfg c_lazy[13] = {
-    {0, 0, 0, 5},       {0, 0, 0, 5},       {0, 0, 0, 5},       {0, 0, 0, 5},
-    {64, 128, 1, 5},    {128, 128, 1, 5},   {128, 258, 1, 5},   {256, 258, 2, 6},
-    {512, 258, 2, 6},   {768, 258, 3, 6},   {1024, 258, 3, 8},  {2048, 258, 3, 8},
-    {4096, 258, 3, 8}};
+    {0, 0, 0, 5, 0},       {0, 0, 0, 5, 0},       {0, 0, 0, 5, 0},       {0, 0, 0, 5, 0},
+    {64, 128, 1, 5, 0},    {128, 128, 1, 5, 0},   {128, 258, 1, 5, 0},   {256, 258, 2, 6, 0},
+    {512, 258, 2, 6, 0},   {768, 258, 3, 6, 0},   {1024, 258, 3, 8, 1},  {2048, 258, 3, 8, 1},
+    {4096, 258, 3, 8, 1}};
 
 struct SmemBytes {
   const uint32_t* w;  // 16-byte aligned shared words
@@ -219,6 +224,44 @@ __device__ __forceinline__ uint32_t dist_sym(uint32_t d) {
   return dc;
 }
 
+// Literal/length and distance histogram of a tile's tokens (all threads):
+// a block-wide max-scan of match ends marks the bytes matches cover, every
+// other byte is a literal.
+__device__ void tile_histogram(const uint32_t* tok_s, uint32_t tl, const SmemBytes& sd, uint32_t off, uint32_t* hist,
+                               uint32_t* scan) {
+  const uint32_t per = (T + blockDim.x - 1) / blockDim.x;
+  const uint32_t i0 = threadIdx.x * per;
+  uint32_t me = 0;
+  for (uint32_t j = 0; j < per; ++j) {
+    const uint32_t i = i0 + j;
+    const uint32_t tk = i < tl ? tok_s[i] : 0;
+    if (tk) me = max(me, i + ((tk >> 16) & 0x1FFu));
+  }
+  uint32_t run = block_max_excl(me, scan);
+  for (uint32_t j = 0; j < per; ++j) {
+    const uint32_t i = i0 + j;
+    if (i >= tl) break;
+    const uint32_t tk = tok_s[i];
+    if (tk) {
+      const uint32_t len = (tk >> 16) & 0x1FFu;
+      atomicAdd(&hist[257 + len_sym(len)], 1u);
+      atomicAdd(&hist[288 + dist_sym(tk & 0xFFFFu)], 1u);
+      run = max(run, i + len);
+    } else if (run <= i) {
+      atomicAdd(&hist[sd.byte(off + i)], 1u);
+    }
+  }
+  __syncthreads();
+}
+
+// Bit cost (1/16 bit) of a token with `count` in a histogram of `total`
+// symbols: log2(total / count), 1..15 bits; unseen symbols cost 2 bits more
+// than the rarest possible.
+__device__ __forceinline__ uint16_t sym_cost(uint32_t count, uint32_t total) {
+  const float b = count ? __log2f(float(total) / float(count)) : __log2f(float(total)) + 2.0f;
+  return uint16_t(16.0f * fminf(fmaxf(b, 1.0f), 15.0f) + 0.5f);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- k_lz
@@ -236,6 +279,9 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
   uint32_t* fm = tok_s + T;
   uint32_t* hist = fm + kFmWords;
   uint32_t* scan = hist + 320;
+  uint16_t* choice = reinterpret_cast<uint16_t*>(scan + 64);  // optimal parse: token length at each position
+  uint16_t* scost = choice + T;                              // symbol costs, 1/16 bit: 0-255 literals, 257+ lengths, 288+ distances
+  uint16_t* lcost = scost + 320;                             // cost of a match length 0..258 (code + extra bits)
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
   if (blockIdx.x >= nruns) return;
@@ -493,32 +539,81 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     }
     __syncthreads();
 
-    // -- covered bytes (max-scan of match ends) and the histogram
-    const uint32_t per = (T + blockDim.x - 1) / blockDim.x;
-    const uint32_t i0 = tid * per;
-    uint32_t me = 0;
-    for (uint32_t j = 0; j < per; ++j) {
-      const uint32_t i = i0 + j;
-      const uint32_t tk = i < tl ? tok_s[i] : 0;
-      if (tk) me = max(me, i + ((tk >> 16) & 0x1FFu));
+    // -- levels 10-12: optimal parse.  Costs come from the histogram of the
+    // lazy parse above; a backward pass finds, for every position, the
+    // cheapest way to the tile end (a literal, or the match found there
+    // shortened by up to 31 bytes), then the path from position 0 is read.
+    if (cfg.opt) {
+      tile_histogram(tok_s, tl, sd, ts - rs, hist, scan);
+      {
+        uint32_t lt = 1, dt = 0;  // totals (EOB counts once)
+        for (uint32_t k = 0; k < 286; ++k) lt += hist[k];
+        for (uint32_t k = 288; k < 318; ++k) dt += hist[k];
+        for (uint32_t k = tid; k < 320; k += blockDim.x)
+          scost[k] = k < 288 ? sym_cost(hist[k], lt) : sym_cost(hist[k], dt > 0 ? dt : 1);
+      }
+      __syncthreads();
+      for (uint32_t k = tid; k < 320; k += blockDim.x) hist[k] = 0;
+      for (uint32_t k = tid; k < 259; k += blockDim.x) {
+        uint32_t li = 0, lne = 0, lev;
+        if (k >= 3) length_code(k, li, lne, lev);
+        lcost[k] = k >= 3 ? uint16_t(scost[257 + li] + 16 * lne) : uint16_t(0);
+      }
+      // per position, before the backward pass: cost[i] = literal cost,
+      // choice[i] = cost of the distance of the match found at i
+      uint32_t* cost = tok_s;  // cost to the tile end, per position (tokens are rebuilt below)
+      for (uint32_t i = tid; i < tl; i += blockDim.x) {
+        cost[i] = scost[sd.byte(ts - rs + i)];
+        uint32_t dc = 0, dne = 0, dev;
+        if (F[i]) dist_code(F[i] & 0xFFFFu, dc, dne, dev);
+        choice[i] = F[i] ? uint16_t(scost[288 + dc] + 16 * dne) : uint16_t(0);
+      }
+      __syncthreads();
+      if (wid == 0) {
+        uint32_t next = 0;  // cost[i + 1]
+        for (int i = int(tl) - 1; i >= 0; --i) {
+          const uint32_t f = F[i];
+          uint32_t best = ((cost[i] + next) << 9) | 1u;
+          if (f) {
+            const uint32_t flen = f >> 16, dcost = choice[i];
+            const uint32_t L = flen - lane;
+            uint32_t key = kAll;
+            if (lane + 3 <= flen) key = ((lcost[L] + dcost + (i + L < tl ? cost[i + L] : 0u)) << 9) | L;
+            best = __reduce_min_sync(kAll, lane == 0 ? min(key, best) : key);
+          }
+          next = best >> 9;
+          __syncwarp();
+          if (lane == 0) {
+            cost[i] = next;
+            choice[i] = uint16_t(best & 511u);
+          }
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t i = 0, nm = 0;
+        while (i < tl) {
+          const uint32_t c = choice[i];
+          if (c >= 3) {
+            tok_s[i] = 0x80000000u | (c << 16) | (F[i] & 0xFFFFu);
+            ++nm;
+            i += c;
+          } else {
+            ++i;
+          }
+        }
+        scan[63] = nm;
+      }
+      __syncthreads();
     }
+
+    // -- covered bytes (max-scan of match ends) and the histogram
     const uint32_t nm = scan[63];
     __syncthreads();
-    uint32_t run = block_max_excl(me, scan);
-    for (uint32_t j = 0; j < per; ++j) {
-      const uint32_t i = i0 + j;
-      if (i >= tl) break;
-      const uint32_t tk = tok_s[i];
-      if (tk) {
-        const uint32_t len = (tk >> 16) & 0x1FFu;
-        atomicAdd(&hist[257 + len_sym(len)], 1u);
-        atomicAdd(&hist[288 + dist_sym(tk & 0xFFFFu)], 1u);
-        run = max(run, i + len);
-      } else if (run <= i) {
-        atomicAdd(&hist[sd.byte(ts - rs + i)], 1u);
-      }
-    }
-    __syncthreads();
+    tile_histogram(tok_s, tl, sd, ts - rs, hist, scan);
     uint32_t* gh = reinterpret_cast<uint32_t*>(wk.scratch + t.hist);
     for (uint32_t i = tid; i < 320; i += blockDim.x) gh[i] = hist[i];
     uint32_t* gt = reinterpret_cast<uint32_t*>(wk.scratch + t.tok);

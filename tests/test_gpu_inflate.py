@@ -68,7 +68,7 @@ def test_errors_like_the_reference(gpu):
         r, _ = raw_call(bytes(c), fmt, len(d))
         assert r == 0
         bad = bytearray(c)
-        bad[-5 if fmt == 1 else -6] ^= 0x40  # checksum byte
+        bad[-2 if fmt == 1 else -6] ^= 0x40  # a byte of the Adler-32 / CRC-32 trailer
         assert raw_call(bytes(bad), fmt, len(d))[0] == DATA_ERROR
         assert raw_call(bytes(c[: len(c) // 2]), fmt, len(d))[0] == DATA_ERROR  # truncated
         assert raw_call(bytes(c), fmt, len(d) - 1)[0] == DATA_ERROR            # output too small
@@ -125,3 +125,18 @@ def test_gzip_members_errors(gpu):
     first_end = len(deflate.compress_gzip_members(d[: 1 << 20], 6, 1 << 20))
     blob[first_end - 8] ^= 1
     assert raw_call(bytes(blob), 2, len(d))[0] == DATA_ERROR
+
+
+def test_header_pattern_inside_member_data(gpu):
+    """A gzip file of 256 KiB or more whose data holds a gzip-header-like
+    pattern: the member scan splits on it, and the file must still decode
+    (as one stream, or member after member)."""
+    d = bytearray(synth.gen(400000, synth.RANDOM, 11))
+    fake = bytes([0x1F, 0x8B, 8, 0, 1, 2, 3, 4, 0, 3]) + b"\xff" * 12
+    d[1000:1000 + len(fake)] = fake
+    d[300000:300000 + len(fake)] = fake
+    d = bytes(d)
+    for blob in (deflate.compress(d, 0, deflate.Format.Gzip),
+                 deflate.compress(d[:200000], 0, deflate.Format.Gzip) + deflate.compress(d[200000:], 0, deflate.Format.Gzip)):
+        assert raw_call(blob, 2, len(d)) == (0, d)
+        assert raw_call(blob, 2, len(d) - 1)[0] in (DATA_ERROR, -2)
