@@ -444,6 +444,7 @@ uint32_t Engine::checksum_device(uint32_t init, const uint8_t* d_data, size_t n,
 }
 
 std::mutex& global_mutex() { static std::mutex m; return m; }
+deflate_allocator g_allocator{};  // set by deflate_set_allocator, never used to allocate
 Engine& global_engine() { static Engine* e = new Engine(); return *e; }
 
 }  // namespace orotb
@@ -459,11 +460,12 @@ struct deflate_parallel_ctx {
 
 extern "C" {
 
-// Kept for ABI compatibility; like the reference, nothing allocates through it.
-static deflate_allocator g_user_alloc{};
+// Kept for ABI compatibility: like the reference (src/api/deflate_api.cpp:75-77)
+// the allocator is stored and nothing allocates through it (device memory
+// never comes from a host allocator).
 void deflate_set_allocator(const deflate_allocator* a) {
-  if (a) g_user_alloc = *a;
-  (void)g_user_alloc;
+  std::lock_guard<std::mutex> lk(global_mutex());
+  g_allocator = a ? *a : deflate_allocator{};
 }
 
 size_t deflate_compress_bound(size_t n, deflate_format f) { return framed_bound(n, int(f)); }
