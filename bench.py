@@ -444,7 +444,7 @@ def main():
 
     # -- plain path: one pass per buffer (device-resident) and deflate_compress per buffer
     plain = None
-    if args.plain_sample > 0:
+    if args.plain_sample > 0 and world == 1:
         idx = sample_indices(sizes, 1 << 62, 3)[:args.plain_sample]
         single = []
         for i in idx:
@@ -494,7 +494,7 @@ def main():
 
     # -- serving: Poisson arrivals through the continuous-batching server
     serving = None
-    if args.serve_requests > 0:
+    if args.serve_requests > 0 and world == 1:  # a one-GPU measurement; scaling runs skip it
         serving = measure_serving(deflate, buf, total, args.serve_requests, args.serve_rate, seed=rank)
 
     # -- CPU baseline: the reference on the host cores (rank 0, N = 1 only)
