@@ -146,7 +146,7 @@ __host__ __device__ inline uint64_t lazy_stream_bytes(uint32_t tile_len) { retur
 // into independent tiles costs no extra token on such data.  One CTA walks a
 // run of kLazyRun consecutive tiles, sliding its window.
 constexpr uint32_t kLazyTile = 16 * 258;
-constexpr uint32_t kLazyRun = 16;
+constexpr uint32_t kLazyRun = 32;
 constexpr uint32_t kLazyWindow = 32768;
 
 }  // namespace orotb

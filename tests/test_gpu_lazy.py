@@ -98,7 +98,7 @@ def test_lazy_window_runs_match_single_tiles(gpu, oracle, level, monkeypatch):
     sizes = [40 << 20, 5 << 20, 4128 * 16 + 1, 4128 * 17, 100]
     bufs = [synth.gen(n, synth.MIXED if i == 0 else i, 40 + i) for i, n in enumerate(sizes)]
     outs = {}
-    for run in ("16", "5", "1"):
+    for run in ("32", "16", "5", "1"):
         monkeypatch.setenv("OROT_B200_LAZY_RUN", run)
         b = gpu.DeviceBatch()
         b.load(b"".join(bufs), sizes, level, gpu.Format.Zlib)
@@ -106,6 +106,7 @@ def test_lazy_window_runs_match_single_tiles(gpu, oracle, level, monkeypatch):
         got = b.sizes()
         outs[run] = [b.output(i, got[i]) for i in range(len(sizes))]
         b.close()
+    assert outs["32"] == outs["1"]
     assert outs["16"] == outs["1"]
     assert outs["5"] == outs["1"]
     for d, out in zip(bufs, outs["16"]):
