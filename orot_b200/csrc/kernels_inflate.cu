@@ -1,19 +1,29 @@
 // kernels_inflate.cu -- DEFLATE decoding (RFC 1951) on sm_100a.
 //
 // Decoding a DEFLATE stream is sequential: each code's length is known only
-// after the previous one is decoded.  The parallel unit is therefore the
+// after the previous one is decoded.  The parallel unit across streams is the
 // stream: one warp per stream, warps take streams from a counter (largest
-// first, so the longest decode starts first).  Inside the warp, lane 0 reads
-// bits and decodes symbols, writing literals itself; the 32 lanes build the
-// Huffman lookup tables together and copy every match together (a copy of
-// length L at distance D reads only bytes before the copy, out[p - D + i % D],
-// so all lanes copy at once even when D < L).
+// first, so the longest decode starts first).
 //
-// Codes are decoded with a 9-bit lookup table (codes up to 9 bits, nearly all
-// symbols of real data) and, for longer codes, the canonical rule of RFC 1951
-// 3.2.2 walked bit by bit: codes of one length are consecutive integers and
-// shorter codes precede longer ones, so per length the code is compared
-// against the first code and the number of codes of that length.
+// Inside the warp the symbols are decoded speculatively, a window of 64 bit
+// offsets at a time: every lane decodes the token that would start at two of
+// the offsets (a literal, the end of the block, or a length code with its
+// extra bits followed by a distance code with its extra bits, at most 48
+// bits), then the warp follows the chain of tokens from the window's first
+// bit with one shuffle per token, writing each literal from one lane and
+// copying each match with all 32 lanes (a copy of length L at distance D reads
+// only bytes before the copy, out[p - D + i % D], so all lanes copy at once
+// even when D < L).  Tokens off the chain are discarded; a window advances by
+// the bits its chain consumed.
+//
+// Codes are looked up in 9-bit tables whose entries carry everything a token
+// needs (code bits, base length or distance, extra bits).  Longer codes (rare
+// in real data, absent from the fixed code) are resolved when the chain
+// reaches them, by the canonical rule of RFC 1951 3.2.2: codes of one length
+// are consecutive integers and shorter codes precede longer ones, so per
+// length the code is compared against the first code and the number of codes
+// of that length.  Block headers (stored lengths, the code-length code and
+// the code lengths of a dynamic block) are read by lane 0.
 //
 // The kernel does not read the zlib / gzip framing; the host strips it and
 // checks the trailer against a checksum of the output (src/formats/*:
@@ -32,6 +42,7 @@ constexpr int kFastBits = 9;
 constexpr uint32_t kFast = 1u << kFastBits;
 constexpr uint32_t kWin = 8192;   // recent output kept in shared memory per warp
 constexpr int kInfWarps = 4;      // warps per CTA
+constexpr uint32_t kSpan = 64;    // bit offsets decoded speculatively per window (two per lane)
 
 // RFC 1951 3.2.5: base lengths / distances and extra bits of symbols 257..285
 // and distance codes 0..29.
@@ -44,10 +55,33 @@ __constant__ uint8_t c_dist_extra[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 
 // order of the code-length code lengths in a dynamic block header (3.2.7)
 __constant__ uint8_t c_cl_order[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
 
-// One Huffman code: lookup table for codes up to 9 bits ((len << 12) | sym,
-// 0 = longer code), code counts per length and the symbols in code order.
+// Lookup-table entries (0: the code is longer than kFastBits or not assigned).
+//   code-length code: [0,4) code bits, [16,32) symbol
+//   literal/length:   [0,4) code bits, [4,6) kind (0 literal, 1 length,
+//                     2 end of block, 3 symbol 286/287), [6,11) code + extra
+//                     bits, [11,14) extra bits, [16,32) literal or base length
+//   distance:         [0,4) code bits, [4,8) extra bits, [8,13) code + extra
+//                     bits, bit 15 symbol 30/31, [16,32) base distance
+enum : uint32_t { kTabCl = 0, kTabLit = 1, kTabDist = 2 };
+
+__device__ __forceinline__ uint32_t make_entry(uint32_t tab, uint32_t s, uint32_t n) {
+  if (tab == kTabCl) return n | (s << 16);
+  if (tab == kTabLit) {
+    if (s < 256) return n | (n << 6) | (s << 16);
+    if (s == 256) return n | (2u << 4) | (n << 6);
+    if (s > 285) return n | (3u << 4) | (n << 6);
+    const uint32_t x = c_len_extra[s - 257];
+    return n | (1u << 4) | ((n + x) << 6) | (x << 11) | (uint32_t(c_len_base[s - 257]) << 16);
+  }
+  if (s > 29) return n | 0x8000u;
+  const uint32_t x = c_dist_extra[s];
+  return n | (x << 4) | ((n + x) << 8) | (uint32_t(c_dist_base[s]) << 16);
+}
+
+// One Huffman code: lookup table, code counts per length and the symbols in
+// code order.
 struct Code {
-  uint16_t* fast;
+  uint32_t* fast;
   uint16_t* count;  // [16]
   uint16_t* sym;    // [nsym]
 };
@@ -56,7 +90,7 @@ struct Code {
 // whose source lies in the window reads shared memory instead of waiting for
 // the bytes this warp has just stored to come back from L2.
 struct WarpMem {
-  uint16_t lfast[kFast], dfast[kFast];
+  uint32_t lfast[kFast], dfast[kFast];
   uint16_t lcount[16], dcount[16];
   uint16_t lsym[288], dsym[32];
   uint16_t first[16], offs[16];  // builder scratch: first code and first index per length
@@ -64,11 +98,13 @@ struct WarpMem {
   uint32_t bad;                  // builder result
   uint8_t win[kWin];             // the last kWin output bytes, at position & (kWin - 1)
 };
+constexpr size_t kInfSmem = sizeof(WarpMem) * kInfWarps;
 
-// Builds `c` from code lengths lens[0..n) (all lanes).  Returns false for an
-// over-subscribed set of lengths; an incomplete set is accepted (a code that
-// is not assigned is reported when it is read).
-__device__ bool build_code(const Code& c, const uint8_t* lens, uint32_t n, WarpMem& m, uint32_t lane) {
+// Builds `c` from code lengths lens[0..n) (all lanes); `tab` selects the
+// entry layout.  Returns false for an over-subscribed set of lengths; an
+// incomplete set is accepted (a code that is not assigned is reported when
+// it is read).
+__device__ bool build_code(const Code& c, const uint8_t* lens, uint32_t n, uint32_t tab, WarpMem& m, uint32_t lane) {
   for (uint32_t i = lane; i < kFast; i += 32) c.fast[i] = 0;
   if (lane == 0) {
     for (int l = 0; l < 16; ++l) c.count[l] = 0;
@@ -95,7 +131,7 @@ __device__ bool build_code(const Code& c, const uint8_t* lens, uint32_t n, WarpM
   }
   __syncwarp();
   if (m.bad) return false;
-  // fill the lookup table: symbol i (in code order) of length l <= 9
+  // fill the lookup table: symbol i (in code order) of length l <= kFastBits
   uint32_t total = 0;
   for (int l = 1; l < 16; ++l) total += c.count[l];
   for (uint32_t i = lane; i < total; i += 32) {
@@ -104,14 +140,16 @@ __device__ bool build_code(const Code& c, const uint8_t* lens, uint32_t n, WarpM
     if (l > uint32_t(kFastBits)) continue;
     const uint32_t code = m.first[l] + (i - m.offs[l]);
     const uint32_t rev = __brev(code) >> (32 - l);  // codes are sent most significant bit first
-    for (uint32_t k = rev; k < kFast; k += 1u << l) c.fast[k] = uint16_t((l << 12) | s);
+    const uint32_t e = make_entry(tab, s, l);
+    for (uint32_t k = rev; k < kFast; k += 1u << l) c.fast[k] = e;
   }
   __syncwarp();
   return true;
 }
 
-// LSB-first bit reader over [p, end); reads whole aligned words (the buffers
-// carry padding after their last byte) and counts bits taken past the end.
+// LSB-first bit reader over [p, end) for the block headers (lane 0); reads
+// whole aligned words (the buffers carry padding after their last byte) and
+// counts bits taken past the end.
 struct BitIn {
   const uint8_t* base;
   uint64_t pos, end;  // byte positions relative to base
@@ -136,17 +174,28 @@ struct BitIn {
     cnt -= n;
     return v;
   }
+  // bits consumed so far
+  __device__ __forceinline__ uint64_t bits() const { return pos * 8 - cnt; }
   // bytes consumed so far
   __device__ __forceinline__ uint64_t used() const { return pos - cnt / 8; }
 };
 
-// Decodes one symbol (lane 0).  Returns 0xFFFF for a code that is not assigned.
+// A reader positioned at bit `p` of the stream.
+__device__ __forceinline__ BitIn bitin_at(const uint8_t* base, uint64_t end, uint64_t p) {
+  BitIn b{base, p >> 3, end, 0, 0};
+  b.refill();
+  b.take(uint32_t(p & 7));
+  return b;
+}
+
+// Decodes one symbol of the code-length code (lane 0).  Returns 0xFFFF for a
+// code that is not assigned.
 __device__ __forceinline__ uint32_t decode(BitIn& b, const Code& c) {
   b.refill();
   const uint32_t e = c.fast[uint32_t(b.buf) & (kFast - 1)];
   if (e) {
-    b.take(e >> 12);
-    return e & 0xFFFu;
+    b.take(e & 15u);
+    return e >> 16;
   }
   int code = 0, first = 0, index = 0;
   for (int l = 1; l < 16; ++l) {
@@ -160,15 +209,92 @@ __device__ __forceinline__ uint32_t decode(BitIn& b, const Code& c) {
   return 0xFFFFu;
 }
 
+// Canonical decode of the code at the low bits of `w` without the table;
+// returns the symbol and its code length, or 0xFFFF for a code that is not
+// assigned.
+__device__ __forceinline__ uint32_t canon_peek(uint64_t w, const uint16_t* count, const uint16_t* sym, uint32_t& n) {
+  int code = 0, first = 0, index = 0;
+  for (int l = 1; l < 16; ++l) {
+    code |= int((w >> (l - 1)) & 1u);
+    const int cnt = count[l];
+    if (code - first < cnt) {
+      n = uint32_t(l);
+      return sym[index + (code - first)];
+    }
+    index += cnt;
+    first = (first + cnt) << 1;
+    code <<= 1;
+  }
+  n = 0;
+  return 0xFFFFu;
+}
+
+// Tokens: [0,6) bits, [6,8) kind (0 literal, 1 match, 2 end of block, 3 not
+// decoded); literal: [8,16) byte; match: [8,17) length, [17,32) distance - 1;
+// not decoded: [8,16) 0 = a code longer than the tables, 1 = invalid code.
+constexpr uint32_t kTokSlow = 3u << 6, kTokBad = (3u << 6) | (1u << 8);
+
+// Decodes the token at the low bits of `w` (up to 48 bits).  Without Slow a
+// code missing from a table gives kTokSlow; with Slow it is decoded by the
+// canonical rule.
+template <bool Slow>
+__device__ __forceinline__ uint32_t token(uint64_t w, const WarpMem& m) {
+  uint32_t e = m.lfast[uint32_t(w) & (kFast - 1)];
+  if (!(e & 15u)) {
+    if (!Slow) return kTokSlow;
+    uint32_t n;
+    const uint32_t s = canon_peek(w, m.lcount, m.lsym, n);
+    if (s == 0xFFFFu) return kTokBad;
+    e = make_entry(kTabLit, s, n);
+  }
+  const uint32_t n = e & 15u, kind = (e >> 4) & 3u;
+  if (kind != 1) return kind == 3 ? kTokBad : (n | (kind << 6) | ((e >> 16) << 8));
+  const uint32_t tot = (e >> 6) & 31u, x = (e >> 11) & 7u;
+  const uint32_t len = (e >> 16) + (uint32_t(w >> n) & ((1u << x) - 1u));
+  const uint64_t w2 = w >> tot;
+  uint32_t d = m.dfast[uint32_t(w2) & (kFast - 1)];
+  if (!(d & 15u)) {
+    if (!Slow) return kTokSlow;
+    uint32_t dn;
+    const uint32_t s = canon_peek(w2, m.dcount, m.dsym, dn);
+    if (s == 0xFFFFu) return kTokBad;
+    d = make_entry(kTabDist, s, dn);
+  }
+  if (d & 0x8000u) return kTokBad;
+  const uint32_t dn = d & 15u, dx = (d >> 4) & 15u;
+  const uint32_t dist = (d >> 16) + (uint32_t(w2 >> dn) & ((1u << dx) - 1u));
+  return (tot + ((d >> 8) & 31u)) | (1u << 6) | (len << 8) | ((dist - 1u) << 17);
+}
+
+// Aligned input word j of a stream whose last bit is at absolute bit `endb`
+// (bits at or past it read as zero).
+__device__ __forceinline__ uint32_t word_at(const uint32_t* a, uint64_t j, uint64_t endb) {
+  const uint64_t b0 = j * 32;
+  if (b0 >= endb) return 0;
+  uint32_t v = __ldg(a + j);
+  if (endb - b0 < 32) v &= (1u << uint32_t(endb - b0)) - 1u;
+  return v;
+}
+
+// 64 bits starting at bit `rel` (< 96) of the five words w0..w4.
+__device__ __forceinline__ uint64_t bits_at(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t w4,
+                                            uint32_t rel) {
+  const uint32_t q = rel >> 5, s = rel & 31u;
+  const uint32_t x0 = q == 0 ? w0 : q == 1 ? w1 : w2;
+  const uint32_t x1 = q == 0 ? w1 : q == 1 ? w2 : w3;
+  const uint32_t x2 = q == 0 ? w2 : q == 1 ? w3 : w4;
+  return (uint64_t(__funnelshift_r(x1, x2, s)) << 32) | __funnelshift_r(x0, x1, s);
+}
+
 }  // namespace
 
 // status: kInfOk, kInfData (corrupt), kInfOutput (output full), kInfInput (input exhausted)
 __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
                                                  InflateJob* jobs, const uint32_t* __restrict__ order, uint32_t njobs,
                                                  uint32_t* counter) {
-  __shared__ WarpMem wm[kInfWarps];
+  extern __shared__ __align__(16) uint8_t inf_smem[];
   const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  WarpMem& m = wm[wid];
+  WarpMem& m = reinterpret_cast<WarpMem*>(inf_smem)[wid];
   const Code lit{m.lfast, m.lcount, m.lsym}, dst{m.dfast, m.dcount, m.dsym};
   for (;;) {
     uint32_t k = 0;
@@ -178,14 +304,21 @@ __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __res
     InflateJob* jp = jobs + order[k];
     const InflateJob job = *jp;
     uint8_t* o = out + job.out_off;
-    BitIn b{in + job.in_off, 0, job.in_len, 0, 0};
+    const uint8_t* base = in + job.in_off;
+    // the stream as aligned words: its first bit is bit s0 of word 0
+    const uint32_t* aw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uint64_t>(base) & ~uint64_t(3));
+    const uint64_t s0 = (reinterpret_cast<uint64_t>(base) & 3) * 8;
+    const uint64_t endb = s0 + job.in_len * 8;
+    uint64_t P = 0;   // bits consumed
     uint64_t op = 0;  // output position
     int32_t status = kInfOk;
     bool last = false;
     while (!last && status == kInfOk) {
       // block header (lane 0 reads, every lane learns the type)
+      BitIn b{base, 0, job.in_len, 0, 0};
       uint32_t hdr = 0;
       if (lane == 0) {
+        b = bitin_at(base, job.in_len, P);
         b.refill();
         hdr = b.take(3);
       }
@@ -204,9 +337,6 @@ __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __res
           len = ln & 0xFFFFu;
           ok = ((ln >> 16) ^ 0xFFFFu) == len;
           src = b.used();  // the bytes left in the buffer are the block's first bytes
-          b.buf = 0;
-          b.cnt = 0;
-          b.pos = src + len;
         }
         len = __shfl_sync(kAll, len, 0);
         ok = __shfl_sync(kAll, ok, 0);
@@ -214,13 +344,14 @@ __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __res
         if (!ok) { status = kInfData; break; }
         if (src + len > job.in_len) { status = kInfInput; break; }
         if (op + len > job.out_cap) { status = kInfOutput; break; }
-        const uint8_t* s = in + job.in_off + src;
+        const uint8_t* s = base + src;
         for (uint32_t i = lane; i < len; i += 32) {
           const uint8_t v = s[i];
           o[op + i] = v;
           m.win[(op + i) & (kWin - 1)] = v;
         }
         op += len;
+        P = (src + len) * 8;
         __syncwarp();
         continue;
       }
@@ -228,8 +359,8 @@ __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __res
       if (type == 1) {
         for (uint32_t i = lane; i < 320; i += 32) m.lens[i] = i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : i < 288 ? 8 : 5;
         __syncwarp();
-        build_code(lit, m.lens, 288, m, lane);
-        build_code(dst, m.lens + 288, 30, m, lane);
+        build_code(lit, m.lens, 288, kTabLit, m, lane);
+        build_code(dst, m.lens + 288, 30, kTabDist, m, lane);
       } else {
         uint32_t hlit = 0, hdist = 0, err = 0;
         if (lane == 0) {
@@ -247,7 +378,7 @@ __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __res
         hlit = __shfl_sync(kAll, hlit, 0);
         hdist = __shfl_sync(kAll, hdist, 0);
         // the code-length code lives in the literal table while the lengths are read
-        if (hlit > 286 || hdist > 30 || !build_code(lit, m.lens + 300, 19, m, lane)) err = 1;
+        if (hlit > 286 || hdist > 30 || !build_code(lit, m.lens + 300, 19, kTabCl, m, lane)) err = 1;
         if (lane == 0 && !err) {
           uint32_t i = 0;
           const uint32_t n = hlit + hdist;
@@ -285,72 +416,105 @@ __global__ void __launch_bounds__(kInfWarps * 32) k_inflate(const uint8_t* __res
         err = __shfl_sync(kAll, err, 0);
         __syncwarp();
         if (err) { status = kInfData; break; }
-        if (!build_code(lit, m.lens, 288, m, lane) || !build_code(dst, m.lens + 288, 30, m, lane)) {
+        if (!build_code(lit, m.lens, 288, kTabLit, m, lane) || !build_code(dst, m.lens + 288, 30, kTabDist, m, lane)) {
           status = kInfData;
           break;
         }
       }
-      // symbols: lane 0 decodes literals until a match or the end of the block
-      for (;;) {
-        uint32_t cmd = 0, len = 0, dist = 0;  // cmd: 0 end of block, 1 match, 2 error
-        int32_t st = kInfOk;
-        if (lane == 0) {
-          for (;;) {
-            const uint32_t sym = decode(b, lit);
-            if (sym < 256) {
-              if (op >= job.out_cap) { st = kInfOutput; cmd = 2; break; }
-              o[op] = uint8_t(sym);
-              m.win[op & (kWin - 1)] = uint8_t(sym);
-              ++op;
-              continue;
-            }
-            if (sym == 256) { cmd = 0; break; }
-            if (sym > 285) { st = kInfData; cmd = 2; break; }
-            b.refill();
-            len = c_len_base[sym - 257] + b.take(c_len_extra[sym - 257]);
-            const uint32_t ds = decode(b, dst);
-            if (ds > 29) { st = kInfData; cmd = 2; break; }
-            b.refill();
-            dist = c_dist_base[ds] + b.take(c_dist_extra[ds]);
-            if (dist > op) { st = kInfData; cmd = 2; break; }
-            if (op + len > job.out_cap) { st = kInfOutput; cmd = 2; break; }
-            cmd = 1;
-            break;
+      P = __shfl_sync(kAll, b.bits(), 0);
+      // symbols, a window of kSpan bit offsets at a time
+      bool block_end = false;
+      while (!block_end && status == kInfOk) {
+        const uint64_t A = s0 + P;  // the window's first bit, counted from aw
+        const uint64_t q = A >> 5;
+        const uint32_t w0 = word_at(aw, q, endb), w1 = word_at(aw, q + 1, endb), w2 = word_at(aw, q + 2, endb),
+                       w3 = word_at(aw, q + 3, endb), w4 = word_at(aw, q + 4, endb);
+        const uint32_t r = uint32_t(A & 31);
+        const uint32_t t_lo = token<false>(bits_at(w0, w1, w2, w3, w4, r + lane), m);
+        const uint32_t t_hi = token<false>(bits_at(w0, w1, w2, w3, w4, r + lane + 32), m);
+        uint32_t cur = 0;  // offset of the next token on the chain
+        uint32_t nl = 0;   // literals decoded but not written yet: lane j holds the j-th in lb
+        uint32_t lb = 0;
+        // bits of the stream from the window's first bit on (capped: every
+        // token on the chain ends before bit kSpan + 48)
+        const uint32_t lim = A >= endb ? 0u : endb - A >= 256 ? 256u : uint32_t(endb - A);
+        while (cur < kSpan) {
+          uint32_t t = __shfl_sync(kAll, cur < 32 ? t_lo : t_hi, cur & 31);
+          uint32_t tb = t & 63u;
+          if (((t >> 6) & 3u) == 0 && cur + tb <= lim && nl < 32) {  // a literal: keep it in lane nl
+            if (lane == nl) lb = t >> 8;
+            ++nl;
+            cur += tb;
+            continue;
           }
-          if (b.used() > job.in_len && st == kInfOk) { st = kInfInput; cmd = 2; }
+          // anything else writes the pending literals first
+          if (nl) {
+            if (op + nl > job.out_cap) { status = kInfOutput; break; }
+            if (lane < nl) {
+              o[op + lane] = uint8_t(lb);
+              m.win[(op + lane) & (kWin - 1)] = uint8_t(lb);
+            }
+            op += nl;
+            nl = 0;
+          }
+          if (((t >> 6) & 3u) == 3u) {
+            if (t != kTokSlow) { status = kInfData; break; }
+            t = token<true>(bits_at(w0, w1, w2, w3, w4, r + cur), m);
+            if (t == kTokBad) { status = kInfData; break; }
+            tb = t & 63u;
+          }
+          const uint32_t kind = (t >> 6) & 3u;
+          if (cur + tb > lim) { status = kInfInput; break; }
+          cur += tb;
+          if (kind == 0) {
+            if (lane == 0) lb = t >> 8;
+            nl = 1;
+            continue;
+          }
+          if (kind == 2) { block_end = true; break; }
+          const uint32_t len = (t >> 8) & 511u, dist = (t >> 17) + 1u;
+          if (dist > op) { status = kInfData; break; }
+          if (op + len > job.out_cap) { status = kInfOutput; break; }
+          __syncwarp();
+          // sources lie before op; in the window unless the copy's own writes
+          // could reach the slots other lanes read (dist + len > kWin)
+          const bool in_win = dist + len <= kWin;
+          for (uint32_t i = lane; i < len; i += 32) {
+            const uint64_t src = op - dist + (i < dist ? i : i % dist);
+            const uint8_t v = in_win ? m.win[src & (kWin - 1)] : o[src];
+            o[op + i] = v;
+            m.win[(op + i) & (kWin - 1)] = v;
+          }
+          __syncwarp();
+          op += len;
         }
-        cmd = __shfl_sync(kAll, cmd, 0);
-        if (cmd != 1) {
-          status = __shfl_sync(kAll, st, 0);
-          break;
+        if (nl && status == kInfOk) {
+          if (op + nl > job.out_cap) {
+            status = kInfOutput;
+          } else {
+            if (lane < nl) {
+              o[op + lane] = uint8_t(lb);
+              m.win[(op + lane) & (kWin - 1)] = uint8_t(lb);
+            }
+            op += nl;
+          }
         }
-        len = __shfl_sync(kAll, len, 0);
-        dist = __shfl_sync(kAll, dist, 0);
-        const uint64_t p0 = __shfl_sync(kAll, op, 0);
         __syncwarp();
-        // sources lie before p0; in the window unless the copy's own writes
-        // could reach the slots other lanes read (dist + len > kWin)
-        const bool in_win = dist + len <= kWin;
-        for (uint32_t i = lane; i < len; i += 32) {
-          const uint64_t src = p0 - dist + (i < dist ? i : i % dist);
-          const uint8_t v = in_win ? m.win[src & (kWin - 1)] : o[src];
-          o[p0 + i] = v;
-          m.win[(p0 + i) & (kWin - 1)] = v;
-        }
-        __syncwarp();
-        if (lane == 0) op += len;
+        P += cur;
       }
-      op = __shfl_sync(kAll, op, 0);
+      __syncwarp();
     }
     if (lane == 0) {
-      if (status == kInfOk && b.used() > job.in_len) status = kInfInput;
+      const uint64_t used = (P + 7) >> 3;
+      if (status == kInfOk && used > job.in_len) status = kInfInput;
       jp->out_len = op;
-      jp->in_used = status == kInfOk ? b.used() : 0;
+      jp->in_used = status == kInfOk ? used : 0;
       jp->status = status;
     }
     __syncwarp();
   }
 }
+
 
 // Compares decoded bytes with the original input, one warp per stream.
 __global__ void __launch_bounds__(256) k_inflate_compare(const uint8_t* __restrict__ a, const uint8_t* __restrict__ b,
@@ -405,7 +569,8 @@ void launch_inflate(const uint8_t* in, uint8_t* out, InflateJob* jobs, const uin
   uint32_t blocks = uint32_t(sms) * 4;  // 4 CTAs of 4 warps per SM (shared memory)
   const uint32_t need = (njobs + kInfWarps - 1) / kInfWarps;
   if (blocks > need) blocks = need;
-  k_inflate<<<blocks, kInfWarps * 32, 0, st>>>(in, out, jobs, order, njobs, counter);
+  cudaFuncSetAttribute(k_inflate, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kInfSmem));
+  k_inflate<<<blocks, kInfWarps * 32, kInfSmem, st>>>(in, out, jobs, order, njobs, counter);
 }
 
 void launch_inflate_compare(const uint8_t* decoded, const uint8_t* ref, InflateJob* jobs, const uint64_t* ref_off,
