@@ -57,9 +57,9 @@ WORKLOAD = "10000 zlib buffers, log-uniform 1 KiB-4 MiB, mixed text/ints/zeros/r
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per input byte of the walk kernel, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on the first 600 buffers of
-# this workload (301.5 MB): 588 MB + 848 MB.  Every term of that traffic is per
+# this workload (301.5 MB): 602 MB + 850 MB.  Every term of that traffic is per
 # byte or per tile, so it is scaled by the input size for the full launch.
-WALK_DRAM_BYTES_PER_INPUT_BYTE = (588.288256e6 + 847.898624e6) / 301540590
+WALK_DRAM_BYTES_PER_INPUT_BYTE = (602.359296e6 + 850.131200e6) / 301540590
 
 
 def parse():
