@@ -406,8 +406,13 @@ deflate_gpu_server* deflate_gpu_server_new(size_t device_budget, int lanes) {
     if (!L) break;
     s.lanes.push_back(L);
     // size the arenas for a full group: one large lazy-level buffer, then
-    // many small fast-level ones (per-buffer tables)
-    if (!lane_warm(*L, s.max_group, 6, s.max_group) || !lane_warm(*L, s.max_group, 1, 4096)) {
+    // many small fast-level ones (per-buffer tables).  The lazy-level buffer
+    // is 1/8 larger than a group: a group of many requests has one partial
+    // tile per request more than one buffer of the same size, and growing an
+    // arena mid-traffic frees device memory, which waits for every pass in
+    // flight (two lanes regrowing once each cost up to 2x in L6 throughput).
+    const uint64_t lazy_warm = s.max_group + s.max_group / 8;
+    if (!lane_warm(*L, lazy_warm, 6, lazy_warm) || !lane_warm(*L, s.max_group, 1, 4096)) {
       for (Lane* X : s.lanes) delete X;
       delete srv;
       return nullptr;
