@@ -140,3 +140,51 @@ def test_header_pattern_inside_member_data(gpu):
                  deflate.compress(d[:200000], 0, deflate.Format.Gzip) + deflate.compress(d[200000:], 0, deflate.Format.Gzip)):
         assert raw_call(blob, 2, len(d)) == (0, d)
         assert raw_call(blob, 2, len(d) - 1)[0] in (DATA_ERROR, -2)
+
+
+def _wrap(raw, data, fmt):
+    if fmt == 0:
+        return raw
+    if fmt == 1:
+        return b"\x78\x9c" + raw + zlib.adler32(data).to_bytes(4, "big")
+    return bytes([0x1F, 0x8B, 8, 0, 0, 0, 0, 0, 0, 0xFF]) + raw + struct.pack("<II", zlib.crc32(data), len(data))
+
+
+@pytest.mark.parametrize("fmt", [0, 1, 2])
+def test_crafted_blocks_and_long_codes(gpu, fmt):
+    """Stored (also empty), fixed and dynamic blocks back to back; dynamic
+    codes of 1 to 15 bits (longer than the 9-bit lookup tables, for literals,
+    lengths and distances) and a 1-bit literal code (64 tokens in a window,
+    32 literals pending at once); every length and distance the history
+    allows (tests/deflate_craft.py)."""
+    from deflate_craft import crafted_stream
+    for seed in range(6):
+        raw, data = crafted_stream(seed)
+        assert deflate.decompress(_wrap(raw, data, fmt), deflate.Format(fmt), len(data)) == data
+
+
+def test_zlib_strategies_and_flushes(gpu):
+    """zlib's filtered, Huffman-only, RLE and fixed strategies, with sync and
+    full flushes (empty stored blocks, byte alignment) between chunks."""
+    skew = bytes(synth.gen(300000, synth.RANDOM, 3)[i] if i % 97 == 0 else 65 for i in range(300000))
+    for d in (synth.gen(300000, synth.MIXED, 12), synth.gen(200000, synth.TEXT, 13), skew):
+        for strategy in (0, 1, 2, 3, 4):
+            for flush in (zlib.Z_NO_FLUSH, zlib.Z_SYNC_FLUSH, zlib.Z_FULL_FLUSH):
+                c = zlib.compressobj(6, zlib.DEFLATED, -15, 9, strategy)
+                z = b""
+                for i in range(0, len(d), 70001):
+                    z += c.compress(d[i:i + 70001]) + (c.flush(flush) if flush != zlib.Z_NO_FLUSH else b"")
+                z += c.flush()
+                assert deflate.decompress(z, deflate.Format.Raw, len(d)) == d, (strategy, flush)
+
+
+def test_truncated_at_every_byte(gpu):
+    """Every proper prefix of a stream fails with DEFLATE_DATA_ERROR (the last
+    block never ends, or the trailer is missing); the whole stream decodes."""
+    from deflate_craft import crafted_stream
+    raw, data = crafted_stream(7, tokens=120)
+    for fmt in (0, 1):
+        blob = _wrap(raw, data, fmt)
+        assert raw_call(blob, fmt, len(data)) == (0, data)
+        for k in range(len(blob)):
+            assert raw_call(blob[:k], fmt, len(data))[0] == DATA_ERROR, (fmt, k)
