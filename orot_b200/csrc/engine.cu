@@ -229,6 +229,22 @@ bool Engine::plan(const std::vector<Job>& jobs) {
     s.ck_count = uint32_t(cks.size()) - s.ck_first;
     streams.push_back(s);
   }
+  // Walkers take tiles longest first: full tiles, then the last (partial)
+  // tiles of the segments by decreasing length, so that a walker which picks
+  // up a tile near the end of the pass finishes soon after the others (one
+  // warp needs about 3 ms for a full 64 KiB tile).  The order does not change
+  // the output: tiles are walked independently and fixed up afterwards.
+  for (const int li : {kWalk12, kWalk14}) {
+    std::vector<uint32_t>& v = lists[li];
+    std::vector<uint32_t> part;
+    size_t nfull = 0;
+    for (const uint32_t x : v) {
+      if (tiles[x].len == T) v[nfull++] = x;
+      else part.push_back(x);
+    }
+    std::stable_sort(part.begin(), part.end(), [&](uint32_t a, uint32_t b) { return tiles[a].len > tiles[b].len; });
+    std::copy(part.begin(), part.end(), v.begin() + nfull);
+  }
   n_pieces = npieces;
   scratch_bytes = align_up(scratch + 256, 256);
 
