@@ -331,7 +331,8 @@ bool Engine::launch(cudaStream_t st) {
     L.counter = counters + g;  // walk: 0/1; fix-up round 1: 4/5 (counter + 4)
     if (L.n_walk) {
       launch_fast(w, L, hbs[g], st, sms, &marks);
-      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 2 : 0) + 1;
+      // k_lastocc; k_carry_scan, k_fix1, k_fix2 for multi-tile segments; k_walk
+      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 3 : 0) + 1;
     }
   }
   if (!lists[kLazyTiles].empty()) {

@@ -165,3 +165,17 @@ def test_device_batch_equals_single_calls(gpu):
             assert b.output(i, got[i]) == single
     assert b.launches() > 0
     b.close()
+
+
+def test_launch_count_matches_the_kernels_of_a_pass(gpu):
+    """deflate_gpu_batch_launches counts every kernel of a pass: at level 1
+    with a multi-tile buffer and zlib framing that is k_lastocc, k_carry_scan,
+    k_walk, k_fix1, k_fix2, k_plan, k_zero, k_join, k_ck_block, k_ck_fold and
+    k_frame (11); raw output drops the two checksum kernels."""
+    d = synth.gen(3 << 20, synth.MIXED, 2)
+    for fmt, want in ((gpu.Format.Zlib, 11), (gpu.Format.Raw, 9)):
+        b = gpu.DeviceBatch()
+        b.load(d, [len(d)], 1, fmt)
+        b.run()
+        assert b.launches() == want
+        b.close()
