@@ -69,7 +69,10 @@ size_t deflate_compress_bound(size_t in_size, deflate_format format);
 /* Replaces deflate_compress, include/orot/deflate.h:72-77.  One DEFLATE
  * block for the whole input; levels 1-3 give byte-identical output to the
  * reference.  Returns the compressed size, or 0 if out_capacity is below
- * deflate_compress_bound() or on any device error. */
+ * deflate_compress_bound() or on any device error.  Positions inside one
+ * block are 32-bit on the device: an input above 4 GiB - 64 KiB returns 0
+ * ("segment larger than 4 GiB"); deflate_parallel_compress, whose chunks are
+ * independent, takes inputs of any size. */
 size_t deflate_compress(const void* in, size_t in_size, void* out, size_t out_capacity, int level,
                         deflate_format format);
 
