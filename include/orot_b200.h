@@ -206,7 +206,9 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
  * request has deflate_compress semantics at its own level and format, so its
  * bytes do not depend on its batch.
  *   submit: `in` and `out` must stay valid until wait returns; returns a
- *           ticket (0 on error).  An `out_capacity` below
+ *           ticket (0 on error, also for a request above 2 GiB: larger
+ *           inputs go through deflate_compress or the batch calls).  An
+ *           `out_capacity` below
  *           deflate_compress_bound() is accepted and makes that request fail
  *           alone if its output does not fit.
  *   wait:   0 done (*out_size, *latency_s = submit to completion), -2 failed,
