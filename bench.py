@@ -483,17 +483,19 @@ def main():
     if not args.no_e2e:
         obound = deflate.packed_bound(sizes, deflate.Format.Zlib)
         outp = torch.empty(obound, dtype=torch.uint8, pin_memory=True).numpy()
-        deflate.compress_pipelined(buf[:total], sizes, args.level, deflate.Format.Zlib, outp)  # warm-up
+        sizes_u64 = np.asarray(sizes, np.uint64)
+        deflate.compress_pipelined(buf[:total], sizes_u64, args.level, deflate.Format.Zlib, outp)  # warm-up
         barrier()
         t0 = time.perf_counter()
         steps_e2e = max(1, min(args.steps, 3))
         packed = 0
         for _ in range(steps_e2e):
-            packed, poffs, psz = deflate.compress_pipelined(buf[:total], sizes, args.level, deflate.Format.Zlib, outp)
+            packed, poffs, psz = deflate.compress_pipelined(buf[:total], sizes_u64, args.level, deflate.Format.Zlib,
+                                                            outp)
         dt = (time.perf_counter() - t0) / steps_e2e
         barrier()
         dt = max_over_ranks(dt)
-        if psz != out_sizes:
+        if psz.tolist() != out_sizes:
             raise SystemExit("end-to-end sizes differ from the device-resident pass")
         e2e = {"value": world * total / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": total,
                "d2h_bytes_per_step": int(comp) + 16 * (len(sizes) + 1), "ms_per_step": dt * 1e3,

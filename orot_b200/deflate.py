@@ -321,22 +321,28 @@ def compress_packed(concat, sizes: Sequence[int], level: int, format: Format, ou
     return r, list(offs), list(szs)
 
 
-def compress_pipelined(concat, sizes: Sequence[int], level: int, format: Format, out, group_bytes: int = 0,
-                       lanes: int = 0) -> tuple[int, list, list]:
-    """deflate_gpu_compress_pipelined; `out` needs packed_bound(sizes) bytes."""
+def compress_pipelined(concat, sizes, level: int, format: Format, out, group_bytes: int = 0,
+                       lanes: int = 0) -> tuple:
+    """deflate_gpu_compress_pipelined; `out` needs packed_bound(sizes) bytes.
+    `sizes` is a sequence of ints or a uint64 numpy array (passed without a
+    copy); returns (end, offsets, sizes) with the stream offsets (count + 1
+    entries) and sizes in `out` as uint64 numpy arrays."""
+    import numpy as np
     L = lib()
     addr, n, keep = _ptr(concat)
     oaddr, on, okeep = _ptr(out)
-    cnt = len(sizes)
-    arr = (ctypes.c_size_t * cnt)(*sizes)
-    offs = (ctypes.c_uint64 * (cnt + 1))()
-    szs = (ctypes.c_size_t * cnt)()
-    r = L.deflate_gpu_compress_pipelined(addr if n else None, arr, cnt, int(level), int(format), oaddr, on, offs, szs,
-                                         int(group_bytes), int(lanes))
+    sz = np.ascontiguousarray(sizes, dtype=np.uint64)
+    cnt = len(sz)
+    offs = np.empty(cnt + 1, np.uint64)
+    szs = np.empty(cnt, np.uint64)
+    p_size = ctypes.POINTER(ctypes.c_size_t)
+    r = L.deflate_gpu_compress_pipelined(addr if n else None, sz.ctypes.data_as(p_size), cnt, int(level), int(format),
+                                         oaddr, on, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                         szs.ctypes.data_as(p_size), int(group_bytes), int(lanes))
     del keep, okeep
     if r == 0:
         raise Error(DEFLATE_BUF_ERROR, "compress_pipelined: " + last_error())
-    return r, list(offs), list(szs)
+    return r, offs, szs
 
 
 class Server:
