@@ -260,12 +260,17 @@ bool Engine::plan(const std::vector<Job>& jobs) {
   off_tiles = put_table(buf, tiles);
   off_ck = put_table(buf, cks);
   // Lazy tiles go to CTAs in runs of consecutive tiles of one segment (the
-  // window slides from tile to tile); runs shorten when there are too few
-  // tiles to give every SM several.
+  // window slides from tile to tile, and every run first builds the links of
+  // its whole window); runs shorten when there are too few tiles to give
+  // every SM several, and keep ~20 runs per SM (one CTA per SM) down to 16
+  // tiles, so that the last wave of runs is a small part of a pass: a 203 MB
+  // pass at level 6 runs 3% faster with runs of 16 than of 32, a 5.1 GB pass
+  // 4% slower.
   if (!lists[kLazySegs].empty()) {
     const uint32_t n = uint32_t(lists[kLazyTiles].size());
+    const uint32_t by_sm = std::max(1u, std::min(kLazyRun, n / (4u * uint32_t(sms))));
     const uint32_t R = lazy_run_override ? lazy_run_override
-                                         : std::max(1u, std::min(kLazyRun, n / (4u * uint32_t(sms))));
+                                         : std::min(by_sm, std::max(16u, n / (20u * uint32_t(sms))));
     for (uint32_t si : lists[kLazySegs]) {
       const Segment& g = segs[si];
       for (uint32_t t = 0; t < g.tile_count; t += R) {
