@@ -79,3 +79,71 @@ def test_host_side_rejections(lib):
     # empty input returns the initial value (test_deflate_simd.cpp:41-42,83)
     assert lib.deflate_crc32(0x1234, None, 0) == 0x1234
     assert lib.deflate_adler32(1, None, 0) == 1
+
+
+def test_more_host_side_rejections(lib):
+    """Argument checks of the other entry points, all answered on the host
+    before any device work (the reference's DEFLATE_PARAM_ERROR, -5, where it
+    has the call; the documented codes of the GPU-only calls otherwise)."""
+    c = ctypes
+    PARAM = -5
+    lib.deflate_decompress.restype = c.c_int
+    lib.deflate_decompress.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.POINTER(c.c_size_t), c.c_int]
+    out = c.create_string_buffer(64)
+    n = c.c_size_t(0)
+    assert lib.deflate_decompress(b"x", 1, out, 64, c.byref(n), 7) == PARAM    # unknown format
+    assert lib.deflate_decompress(None, 5, out, 64, c.byref(n), 0) == PARAM    # input pointer missing
+    assert lib.deflate_decompress(b"x", 1, None, 64, c.byref(n), 0) == PARAM   # output pointer missing
+
+    lib.deflate_stream_new.restype = c.c_void_p
+    lib.deflate_stream_new.argtypes = [c.c_int, c.c_int]
+    lib.deflate_stream_free.argtypes = [c.c_void_p]
+    lib.deflate_stream_compress.restype = c.c_int
+    lib.deflate_stream_compress.argtypes = [c.c_void_p, c.POINTER(c.c_void_p), c.POINTER(c.c_size_t),
+                                            c.POINTER(c.c_void_p), c.POINTER(c.c_size_t), c.c_int]
+    assert not lib.deflate_stream_new(6, 9)
+    s = lib.deflate_stream_new(6, 1)
+    assert s
+    nin, ain = c.c_void_p(None), c.c_size_t(0)
+    nout, aout = c.c_void_p(c.addressof(out)), c.c_size_t(64)
+    assert lib.deflate_stream_compress(None, c.byref(nin), c.byref(ain), c.byref(nout), c.byref(aout), 0) == PARAM
+    assert lib.deflate_stream_compress(s, None, c.byref(ain), c.byref(nout), c.byref(aout), 0) == PARAM
+    assert lib.deflate_stream_compress(s, c.byref(nin), c.byref(ain), c.byref(nout), c.byref(aout), 9) == PARAM
+    ain.value = 10  # input announced without a pointer
+    assert lib.deflate_stream_compress(s, c.byref(nin), c.byref(ain), c.byref(nout), c.byref(aout), 0) == PARAM
+    lib.deflate_stream_free(s)
+    lib.deflate_stream_free(None)
+
+    lib.deflate_gpu_compress_noalloc.restype = c.c_int
+    lib.deflate_gpu_compress_noalloc.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.c_int, c.c_int,
+                                                 c.c_void_p, c.c_void_p]
+    fake = 4096  # never dereferenced: every case below is rejected first
+    assert lib.deflate_gpu_compress_noalloc(fake, 10, None, 64, 1, 0, fake, None) == -1          # no output
+    assert lib.deflate_gpu_compress_noalloc(fake, 10, fake, 64, 1, 5, fake, None) == -1          # format
+    assert lib.deflate_gpu_compress_noalloc(fake, (1 << 20) + 1, fake, 1 << 22, 1, 0, fake, None) == -2
+    assert lib.deflate_gpu_compress_noalloc(fake, 10, fake, 64, 6, 0, fake, None) == -3          # level
+    assert lib.deflate_gpu_compress_noalloc(fake, 1000, fake, 1000, 1, 0, fake, None) == -4      # capacity
+
+    lib.deflate_gpu_parallel_shard.restype = c.c_int
+    lib.deflate_gpu_parallel_shard.argtypes = [c.c_void_p, c.c_size_t, c.c_int, c.c_int, c.c_size_t, c.c_int,
+                                               c.c_void_p, c.c_size_t, c.POINTER(c.c_size_t), c.POINTER(c.c_uint32)]
+    ck = c.c_uint32(0)
+    assert lib.deflate_gpu_parallel_shard(b"abc", 3, 6, 0, 0, 1, None, 64, c.byref(n), c.byref(ck)) == -1
+    assert lib.deflate_gpu_parallel_shard(b"abc", 3, 6, 4, 0, 1, out, 64, c.byref(n), c.byref(ck)) == -1
+
+    lib.deflate_gpu_batch_load.restype = c.c_int
+    lib.deflate_gpu_batch_load.argtypes = [c.c_void_p, c.c_void_p, c.POINTER(c.c_size_t), c.c_size_t, c.c_int, c.c_int,
+                                           c.c_int, c.c_size_t]
+    lib.deflate_gpu_batch_run.restype = c.c_int
+    lib.deflate_gpu_batch_run.argtypes = [c.c_void_p, c.c_void_p, c.c_int]
+    assert lib.deflate_gpu_batch_load(None, b"abc", None, 0, 1, 0, 0, 0) == -1
+    assert lib.deflate_gpu_batch_run(None, None, 0) == -1
+
+    lib.deflate_gpu_server_submit.restype = c.c_uint64
+    lib.deflate_gpu_server_submit.argtypes = [c.c_void_p, c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.c_int,
+                                              c.c_int]
+    lib.deflate_gpu_server_wait.restype = c.c_int
+    lib.deflate_gpu_server_wait.argtypes = [c.c_void_p, c.c_uint64, c.POINTER(c.c_size_t), c.POINTER(c.c_double),
+                                            c.c_double]
+    assert lib.deflate_gpu_server_submit(None, b"abc", 3, out, 64, 1, 0) == 0
+    assert lib.deflate_gpu_server_wait(None, 1, None, None, 0.0) == -1
