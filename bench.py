@@ -14,17 +14,34 @@ Reported (one JSON line from rank 0):
   e2e        the same through deflate_gpu_compress_pipelined from pinned host
              memory: host->device copies, kernels, packing and the
              device->host copies of every compressed stream inside the timing
-             (groups of buffers in flight so copies overlap kernels);
+             (groups of buffers in flight so copies overlap kernels); and the
+             same call from pageable host memory;
   plain      one pass per buffer on a sample (device-resident and through
              deflate_compress), the comparison the batch is measured against;
-  roofline   the dominant kernel phase against the measured HBM copy peak;
+  roofline   the dominant kernel phase against the measured HBM copy peak and
+             against the SM issue rate (its ncu instruction count);
   cpu_baseline  the reference's own deflate_compress (oracle/_ref) on the
              host cores over a bounded sample;
-  serving    Poisson arrivals (2,000 requests/s, 4 KiB-16 MiB, 70% level 1 /
-             30% level 6, raw) through the continuous-batching server: p50/p99
-             latency and sustained GB/s; then the server's capacity (the
-             trace submitted at once; mixed, level 1 and level 6) beside the
-             plain path.
+  threads16  deflate_compress called from 16 host threads at once on a 1 GiB
+             random sample of the buffers, beside the reference's own
+             deflate_compress on the same sample and thread count;
+  configs    the other configurations, each with a device-resident value,
+             an end-to-end value through orot's own C entry point from
+             pageable host memory, its roofline and the reference's entry
+             point on the host cores: 16 MiB Zipf text, raw, level 1, whole
+             buffer (reference: deflate_compress, one thread); 256 MiB mixed
+             data, gzip, level 6, 128 KiB chunks (reference:
+             deflate_parallel_compress on all host threads); 1 GiB random,
+             8-byte periodic with 1% flips and Zipf text, raw, level 9,
+             256 KiB chunks (reference: deflate_parallel_compress on all host
+             threads over the first 64 MiB);
+  serving    20,000 requests with Poisson arrivals (2,000 requests/s, 4 KiB-
+             16 MiB, 70% level 1 / 30% level 6, raw) through the
+             continuous-batching server: p50/p99 latency and sustained GB/s,
+             every result compared with its single deflate_compress output;
+             then the server's capacity (the first 2,000 requests submitted at
+             once; mixed, level 1 and level 6) beside the plain path on a
+             random sample of 300 of them.
   device_verify  every stream of the batch decoded by the GPU inflate and
              compared with its input on the device (wall time of a second
              call, and of the first, which also allocates the decode arena;
@@ -74,7 +91,10 @@ def parse():
     ap.add_argument("--level", type=int, default=1)
     ap.add_argument("--plain-sample", type=int, default=300)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-requests", type=int, default=20000)
+    ap.add_argument("--serve-capacity-requests", type=int, default=2000)
+    ap.add_argument("--no-configs", action="store_true", help="skip the whole-buffer, parallel and stress legs")
+    ap.add_argument("--no-threads", action="store_true", help="skip the 16-thread deflate_compress leg")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     return ap.parse_args()
@@ -245,13 +265,58 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- serving
-def _serve(deflate, srv, buf, trace, gaps):
+class OutRing:
+    """Output space for served requests, reused in submission order: a
+    request's region is handed out only after every request that held it has
+    been collected (collection runs in submission order too)."""
+
+    def __init__(self, nbytes: int):
+        self.buf = np.empty(nbytes, np.uint8)
+        self.head = 0          # next free byte (monotonic)
+        self.regions = []      # monotonic starts of the requests not yet collected, oldest first
+
+    def take(self, n: int, collect_oldest):
+        """Ring offsets [lo, hi) for n bytes; collects the oldest requests
+        first while they still hold any of that space."""
+        n = (n + 63) & ~63
+        size = self.buf.size
+        assert n <= size
+        start = self.head  # monotonic byte position
+        if start % size + n > size:  # does not fit before the ring's end: start over at its beginning
+            start += size - start % size
+        # the ring bytes of [start, start + n) were last handed out as
+        # [start - size, start + n - size); every request starting there must be collected
+        while self.regions and self.regions[0] < start + n - size:
+            collect_oldest()
+        self.head = start + n
+        self.regions.append(start)
+        o = start % size
+        return o, o + n
+
+
+def _serve(deflate, srv, buf, trace, gaps, ring, expect=None):
     """Submits the trace (arrival gaps in seconds, or None for all at once)
-    and waits for every result; returns latencies (s) and the makespan from
-    first submission to last completion."""
-    sizes, levels, starts, outs, ooff = trace
+    and collects every result; returns latencies (s), the makespan from first
+    submission to last completion, and the results' CRC-32s.  With `expect`
+    (the CRC-32 and size of each request's single deflate_compress output),
+    every result is compared as it is collected."""
+    sizes, levels, starts = trace
     n = len(sizes)
-    tickets = [0] * n
+    lat = np.zeros(n)
+    crcs = [0] * n
+    pending = []  # (index, ticket, lo, hi) in submission order
+
+    def collect_oldest():
+        i, t, lo, hi = pending.pop(0)
+        ring.regions.pop(0)
+        o, l = srv.wait(t, timeout=600)
+        if o is None:
+            raise SystemExit(f"served request {i} failed")
+        lat[i] = l
+        crcs[i] = (zlib.crc32(o), len(o))
+        if expect is not None and crcs[i] != expect[i]:
+            raise SystemExit(f"served request {i} differs from its single deflate_compress call")
+
     t0 = time.perf_counter()
     due = t0
     for i in range(n):
@@ -260,85 +325,299 @@ def _serve(deflate, srv, buf, trace, gaps):
             now = time.perf_counter()
             if due > now:
                 time.sleep(due - now)
-        tickets[i] = srv.submit(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw,
-                                out=outs[ooff[i]:ooff[i + 1]])
-    lat = []
-    for i in range(n):
-        o, l = srv.wait(tickets[i], timeout=600)
-        if o is None:
-            raise SystemExit(f"served request {i} failed")
-        lat.append(l)
-    return np.array(lat), time.perf_counter() - t0
+        cap = deflate.compress_bound(sizes[i], deflate.Format.Raw)
+        lo, hi = ring.take(cap, collect_oldest)
+        t = srv.submit(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw, out=ring.buf[lo:hi])
+        pending.append((i, t, lo, hi))
+    while pending:
+        collect_oldest()
+    return lat, time.perf_counter() - t0, crcs
 
 
-def _plain(deflate, buf, trace, k):
-    """The same requests through deflate_compress, one call after another
-    (service time with no queueing)."""
-    sizes, levels, starts = trace[0], trace[1], trace[2]
+def _single_outputs(L, buf, trace, idx, threads=16):
+    """(CRC-32, size) of every request's single deflate_compress output, from
+    `threads` host threads calling the C ABI at once."""
+    sizes, levels, starts = trace
+    base = buf.ctypes.data
+    local = threading.local()
+
+    def one(i):
+        n = sizes[i]
+        cap = n + (n >> 12) + (n >> 14) + (n >> 25) + 13
+        o = getattr(local, "out", None)
+        if o is None or o.size < cap:
+            o = local.out = np.empty(max(cap, 16 << 20), np.uint8)
+        r = L.deflate_compress(base + starts[i], n, o.ctypes.data, cap, levels[i], 0)
+        if r == 0:
+            raise SystemExit(f"deflate_compress failed on request {i}")
+        return zlib.crc32(o[:r]), int(r)
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(one, idx))
+
+
+def _plain(L, buf, trace, idx):
+    """The requests idx through deflate_compress, one call after another on
+    one thread (service time with no queueing)."""
+    sizes, levels, starts = trace
+    base = buf.ctypes.data
+    out = np.empty(max(deflate_bound(max(sizes[i] for i in idx)), 16), np.uint8)
     pl = []
     tp = time.perf_counter()
-    for i in range(k):
+    for i in idx:
         a = time.perf_counter()
-        deflate.compress(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw)
+        if L.deflate_compress(base + starts[i], sizes[i], out.ctypes.data, out.size, levels[i], 0) == 0:
+            raise SystemExit("deflate_compress failed")
         pl.append(time.perf_counter() - a)
     tp = time.perf_counter() - tp
-    return {"requests": k, "GBps": sum(sizes[:k]) / tp / 1e9,
-            "p50_ms": float(np.percentile(np.array(pl) * 1e3, 50)),
+    nb = sum(sizes[i] for i in idx)
+    return {"requests": len(idx), "GBps": nb / tp / 1e9, "p50_ms": float(np.percentile(np.array(pl) * 1e3, 50)),
             "p99_ms": float(np.percentile(np.array(pl) * 1e3, 99))}
 
 
-def measure_serving(deflate, buf, total, count, rate, seed=0):
+def deflate_bound(n: int) -> int:
+    return n + (n >> 12) + (n >> 14) + (n >> 25) + 13
+
+
+def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
     """Serving: raw DEFLATE requests, sizes log-uniform in 4 KiB-16 MiB, cut
     from the mixed workload buffer, through the continuous-batching server
     (16 GiB device budget).
-      open_loop   Poisson arrivals at `rate` requests/s, 70% level 1 / 30%
-                  level 6: p50/p99 latency (submission to completion, timed by
-                  the server) and sustained GB/s (bytes over first submission
-                  to last completion; bounded by the offered rate).
-      capacity    the same trace submitted at once, and the level-1-only and
-                  level-6-only variants: the sustained GB/s the server reaches
-                  when requests queue, beside the plain path (one
-                  deflate_compress per request) on a prefix of the same trace.
-    A sample of served results is checked byte for byte against single
-    deflate_compress calls."""
+      open_loop   `count` requests with Poisson arrivals at `rate` requests/s,
+                  70% level 1 / 30% level 6: p50/p99 latency (submission to
+                  completion, timed by the server) and sustained GB/s (bytes
+                  over first submission to last completion; bounded by the
+                  offered rate).  Every result is compared (CRC-32 and size)
+                  with the same request's single deflate_compress output.
+      capacity    the first `cap_count` requests of the trace submitted at
+                  once (mixed, level-1-only and level-6-only): the sustained
+                  GB/s the server reaches when requests queue, beside the
+                  plain path (one deflate_compress after another) on a random
+                  sample of 300 requests of the same trace."""
     from orot_b200 import synth
+    L = deflate.lib()
     rng = np.random.default_rng(13 + seed)
     sizes = [int(x) for x in synth.loguniform_sizes(count, 4096, 16 << 20, 13 + seed)]
     mix = [1 if u < 0.7 else 6 for u in rng.random(count)]
     starts = [int(rng.integers(0, max(1, total - n))) for n in sizes]
     gaps = rng.exponential(1.0 / rate, count)
-    caps = [deflate.compress_bound(n, deflate.Format.Raw) for n in sizes]
-    outs = np.empty(sum(caps), np.uint8)
-    ooff = np.concatenate([[0], np.cumsum(caps)])
     nbytes = sum(sizes)
+    trace = (sizes, mix, starts)
+    t0 = time.perf_counter()
+    expect = _single_outputs(L, buf, trace, range(count))
+    single_s = time.perf_counter() - t0
     srv = deflate.Server(device_budget=16 << 30, lanes=3)
+    ring = OutRing(6 << 30)
     res = {"requests": count, "rate_req_s": rate, "offered_GBps": nbytes / gaps.sum() / 1e9,
-           "levels": "70% L1 / 30% L6", "format": "raw", "sizes": "log-uniform 4 KiB-16 MiB", "budget_GiB": 16}
-    trace = (sizes, mix, starts, outs, ooff)
-    lat, span = _serve(deflate, srv, buf, trace, gaps)
-    for i in range(0, count, max(1, count // 25)):
-        ref = deflate.compress(buf[starts[i]:starts[i] + sizes[i]], mix[i], deflate.Format.Raw)
-        if outs[ooff[i]:ooff[i] + len(ref)].tobytes() != ref:
-            raise SystemExit(f"served request {i} differs from deflate_compress")
+           "duration_s": float(gaps.sum()), "bytes": nbytes, "levels": "70% L1 / 30% L6", "format": "raw",
+           "sizes": "log-uniform 4 KiB-16 MiB", "budget_GiB": 16}
+    lat, span, _ = _serve(deflate, srv, buf, trace, gaps, ring, expect)
     lat_ms = lat * 1e3
     res["open_loop"] = {"sustained_GBps": nbytes / span / 1e9, "p50_ms": float(np.percentile(lat_ms, 50)),
-                        "p99_ms": float(np.percentile(lat_ms, 99))}
-    k = min(count, 200)
+                        "p99_ms": float(np.percentile(lat_ms, 99)), "p999_ms": float(np.percentile(lat_ms, 99.9)),
+                        "max_ms": float(lat_ms.max()), "verified": count,
+                        "verify": "every result equals its single deflate_compress output (CRC-32 and size)"}
     cap = {}
-    for name, lv in (("mix", mix), ("L1", [1] * count), ("L6", [6] * count)):
-        tr = (sizes, lv, starts, outs, ooff)
-        lat, span = _serve(deflate, srv, buf, tr, None)
-        plain = _plain(deflate, buf, tr, k)
-        cap[name] = {"GBps": nbytes / span / 1e9, "p50_ms": float(np.percentile(lat * 1e3, 50)),
+    k = min(cap_count, count)
+    sample = sorted(np.random.default_rng(77 + seed).choice(k, size=min(300, k), replace=False).tolist())
+    for name, lv in (("mix", mix[:k]), ("L1", [1] * k), ("L6", [6] * k)):
+        tr = (sizes[:k], lv, starts[:k])
+        exp = expect[:k] if name == "mix" else None
+        lat, span, _ = _serve(deflate, srv, buf, tr, None, ring, exp)
+        plain = _plain(L, buf, tr, sample)
+        kb = sum(sizes[:k])
+        cap[name] = {"requests": k, "GBps": kb / span / 1e9, "p50_ms": float(np.percentile(lat * 1e3, 50)),
                      "p99_ms": float(np.percentile(lat * 1e3, 99)), "plain": plain,
-                     "vs_plain": nbytes / span / 1e9 / plain["GBps"]}
+                     "vs_plain": kb / span / 1e9 / plain["GBps"]}
     passes, inflight = srv.stats()
     srv.close()
     res["capacity"] = cap
     res["passes"] = passes
     res["max_passes_in_flight"] = inflight
-    res["plain_note"] = "one deflate_compress per request, back to back, on the first 200 requests"
+    res["plain_note"] = ("one deflate_compress per request, back to back on one thread, on a random sample of 300 "
+                         f"of the first {k} requests")
+    res["single_call_reference_s"] = single_s
     return res
+
+
+# ---------------------------------------------------------------- the other configurations
+# ncu figures of the two dominant kernels (profiles/): warp instructions per
+# input byte, for the issue-rate roofline (4 warp instructions per SM cycle).
+WARP_INST_PER_BYTE = {"walk": 10.5, "lazy_match": 89.0}
+PHASE_KERNEL = {"walk": "k_walk", "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
+                "hash_carry": "k_lastocc + k_carry_scan", "fixup": "k_fix1 + k_fix2", "join": "k_join",
+                "checksum": "k_ck_block + k_ck_fold", "plan": "k_plan + k_zero"}
+
+
+def roofline_of(phases, nbytes, comp, sm_mhz, sms):
+    """Dominant phase of a pass against the HBM copy peak and, where ncu gave
+    its instruction count, against the SM issue rate."""
+    dom = max(phases, key=phases.get)
+    peak, kind = measured_hbm()
+    ms = phases[dom]
+    achieved = (nbytes + comp) / (ms / 1e3) / 1e9
+    r = {"bound": "hbm", "kernel": PHASE_KERNEL.get(dom, dom), "dominant_phase": dom, "achieved": achieved,
+         "peak": peak, "unit": UNIT, "frac": achieved / peak, "peak_source": kind,
+         "phase_ms": {k: round(v, 3) for k, v in phases.items() if v > 0}}
+    if dom in WARP_INST_PER_BYTE and sm_mhz:
+        inst_rate = WARP_INST_PER_BYTE[dom] * nbytes / (ms / 1e3)      # warp instructions / s
+        issue_peak = sms * 4 * sm_mhz * 1e6
+        r["issue"] = {"warp_inst_per_input_byte": WARP_INST_PER_BYTE[dom], "achieved_warp_inst_per_s": inst_rate,
+                      "peak_warp_inst_per_s": issue_peak, "frac": inst_rate / issue_peak,
+                      "note": "instructions per byte from the kernel's ncu capture; peak = SMs x 4 x median SM clock"}
+    return r
+
+
+def load_reference():
+    """The reference built from its sources (oracle/_ref), for the CPU arms."""
+    path = os.path.join(ROOT, "oracle", "_ref", "liborot_ref.so")
+    L = ctypes.CDLL(path)
+    c = ctypes
+    L.deflate_compress.restype = c.c_size_t
+    L.deflate_compress.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t, c.c_int, c.c_int]
+    L.deflate_parallel_new.restype = c.c_void_p
+    L.deflate_parallel_new.argtypes = [c.c_int, c.c_int, c.c_int, c.c_size_t]
+    L.deflate_parallel_free.argtypes = [c.c_void_p]
+    L.deflate_parallel_compress.restype = c.c_size_t
+    L.deflate_parallel_compress.argtypes = [c.c_void_p, c.c_void_p, c.c_size_t, c.c_void_p, c.c_size_t]
+    return L
+
+
+def cpu_reference(data: np.ndarray, level, fmt, parallel, block, threads, reps=2):
+    """The reference's own entry point on the host cores: deflate_compress on
+    one thread (whole buffer) or deflate_parallel_compress with `threads`
+    workers.  Returns (GB/s, compressed size) of the best of `reps` runs."""
+    L = load_reference()
+    n = data.size
+    cap = 2 * n + (1 << 20)
+    out = np.empty(cap, np.uint8)
+    best, size = 1e30, 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        if parallel:
+            ctx = L.deflate_parallel_new(level, fmt, threads, block)
+            r = L.deflate_parallel_compress(ctx, data.ctypes.data, n, out.ctypes.data, cap)
+            L.deflate_parallel_free(ctx)
+        else:
+            r = L.deflate_compress(data.ctypes.data, n, out.ctypes.data, cap, level, fmt)
+        best = min(best, time.perf_counter() - t0)
+        size = int(r)
+    return n / best / 1e9, size
+
+
+def measure_config(deflate, name, data: np.ndarray, level, fmt, parallel, block, stream, sh, steps, cpu_bytes,
+                   cpu_threads, sm_mhz, sms):
+    """One buffer compressed by deflate_compress (whole) or the pigz-style
+    parallel path: device-resident passes (graph replay, CUDA events), the
+    same call end to end through the C ABI from host memory, the on-chip
+    roofline of its dominant kernel, a zlib round trip of the output, and the
+    reference's own entry point on the host cores."""
+    import torch
+    L = deflate.lib()
+    n = data.size
+    b = deflate.DeviceBatch()
+    b.load(data, [n], level, deflate.Format(fmt), parallel=parallel, block_size=block)
+    for _ in range(2):
+        b.run(stream=sh, graph=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        b.run(stream=sh, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    comp = b.sizes()[0]
+    out = b.output(0, comp)
+    if zlib.decompress(out, {0: -15, 1: 15, 2: 31}[fmt]) != data.tobytes():
+        raise SystemExit(f"{name}: output does not round-trip under zlib")
+    b.profile(True)
+    b.run(stream=sh)
+    torch.cuda.synchronize()
+    phases = b.phase_ms()
+    b.profile(False)
+    launches = b.launches()
+    b.close()
+    # end to end through the C ABI: pageable host input and output, the
+    # library's own staging and copies inside the timing
+    cap = 2 * n + (1 << 20)
+    host_out = np.empty(cap, np.uint8)
+    if parallel:
+        ctx = L.deflate_parallel_new(level, fmt, 0, block)
+
+        def call():
+            return L.deflate_parallel_compress(ctx, data.ctypes.data, n, host_out.ctypes.data, cap)
+    else:
+        def call():
+            return L.deflate_compress(data.ctypes.data, n, host_out.ctypes.data, cap, level, fmt)
+    call()
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r = call()
+    e2e_s = (time.perf_counter() - t0) / reps
+    if parallel:
+        L.deflate_parallel_free(ctx)
+    if r != comp or host_out[:r].tobytes() != out:
+        raise SystemExit(f"{name}: the C ABI call differs from the device-resident pass")
+    res = {"value": n / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms, "bytes": n, "ratio": comp / n,
+           "gpu_launches_per_step": launches,
+           "e2e": {"value": n / e2e_s / 1e9, "unit": UNIT, "ms_per_step": e2e_s * 1e3, "h2d_bytes_per_step": n,
+                   "d2h_bytes_per_step": int(comp),
+                   "api": ("deflate_parallel_compress" if parallel else "deflate_compress") +
+                          " (pageable host buffers)"},
+           "roofline": roofline_of(phases, n, comp, sm_mhz, sms)}
+    try:
+        sample = data[:cpu_bytes] if cpu_bytes < n else data
+        v, csize = cpu_reference(sample, level, fmt, parallel, block, cpu_threads)
+        res["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1 if not parallel else cpu_threads,
+                               "kind": "reference",
+                               "sample": (f"first {sample.size >> 20} MiB of the input" if sample.size < n
+                                          else "the whole input") + ", " +
+                                         ("deflate_parallel_compress, num_threads = %d" % cpu_threads if parallel
+                                          else "deflate_compress on one thread"),
+                               "ratio": csize / sample.size}
+        res["vs_cpu_baseline"] = res["e2e"]["value"] / v
+        if sample.size == n:
+            res["size_vs_reference"] = comp / csize
+    except OSError:
+        res["cpu_baseline"] = None
+    return res
+
+
+def measure_threads(deflate, buf, sizes, offs, level, threads, sample_bytes):
+    """deflate_compress from `threads` host threads at once over a random
+    sample of the batch's buffers (zlib), each thread with its own output
+    buffer: what a multithreaded program gets from the drop-in entry point.
+    The reference's own deflate_compress runs the same sample on the same
+    number of threads."""
+    L = deflate.lib()
+    idx = sample_indices(sizes, sample_bytes, 31)
+    base = buf.ctypes.data
+    local = threading.local()
+
+    def one(i):
+        n = sizes[i]
+        cap = n + (n >> 12) + (n >> 14) + (n >> 25) + 19
+        o = getattr(local, "out", None)
+        if o is None:
+            o = local.out = np.empty((4 << 20) + (1 << 16), np.uint8)
+        r = L.deflate_compress(base + int(offs[i]), n, o.ctypes.data, cap, level, 1)
+        if r == 0:
+            raise SystemExit("deflate_compress failed")
+        return int(r)
+
+    with cf.ThreadPoolExecutor(threads) as ex:
+        list(ex.map(one, idx[:threads * 4]))  # warm every engine
+        t0 = time.perf_counter()
+        outs = list(ex.map(one, idx))
+        dt = time.perf_counter() - t0
+    nb = sum(sizes[i] for i in idx)
+    ref, _, _, _, kind = cpu_sample_rate(buf, sizes, offs, idx, level, threads)
+    return {"value": nb / dt / 1e9, "unit": UNIT, "threads": threads, "buffers": len(idx), "bytes": nb,
+            "ratio": sum(outs) / nb, "api": "deflate_compress (pageable host buffers), one call per buffer",
+            "reference": {"value": ref, "unit": UNIT, "threads": threads, "kind": kind},
+            "vs_reference": nb / dt / 1e9 / ref}
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -437,16 +716,11 @@ def main():
         for k, v in b.phase_ms().items():
             phases[k] = phases.get(k, 0.0) + v / nprof
     b.profile(False)
-    dom = max(phases, key=phases.get)
-    peak, peak_kind = measured_hbm()
-    algo_bytes = total + comp  # input read once + compressed bits written once
-    walk_ms = phases.get("walk", 0.0)
-    achieved = algo_bytes / (walk_ms / 1e3) / 1e9 if walk_ms > 0 else None
-    traffic = (WALK_DRAM_BYTES_PER_INPUT_BYTE * total) if WALK_DRAM_BYTES_PER_INPUT_BYTE else None
-    roofline = {"bound": "hbm", "kernel": "k_walk (fast-level LZ77 + fixed Huffman)", "achieved": achieved,
-                "peak": peak, "unit": UNIT, "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "peak_source": peak_kind, "dominant_phase": dom,
-                "phase_ms": {k: round(v, 3) for k, v in phases.items() if v > 0}}
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    roofline = roofline_of(phases, total, comp, clocks.get("sm_mhz"), sms)
+    roofline["traffic"] = WALK_DRAM_BYTES_PER_INPUT_BYTE * total if roofline["dominant_phase"] == "walk" else None
+    roofline["traffic_note"] = "ncu DRAM bytes per input byte of the walk kernel on a 301.5 MB slice, scaled"
     b.close()
 
     # -- plain path: one pass per buffer (device-resident) and deflate_compress per buffer
@@ -478,7 +752,7 @@ def main():
         plain = {"value": pbytes / (pms / 1e3) / 1e9, "e2e": pbytes / pe2e / 1e9, "unit": UNIT,
                  "sample_buffers": len(idx), "sample_bytes": pbytes}
 
-    # -- end to end through the public API (pinned host buffers)
+    # -- end to end through the public API (pinned host buffers; then pageable)
     e2e = None
     if not args.no_e2e:
         obound = deflate.packed_bound(sizes, deflate.Format.Zlib)
@@ -500,11 +774,51 @@ def main():
         e2e = {"value": world * total / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": total,
                "d2h_bytes_per_step": int(comp) + 16 * (len(sizes) + 1), "ms_per_step": dt * 1e3,
                "api": "deflate_gpu_compress_pipelined (pinned host buffers, 512 MiB groups, 4 passes in flight)"}
+        if world == 1:
+            # the same call from pageable (not pinned) input and output memory
+            pin = np.empty(total, np.uint8)
+            pin[:] = buf[:total]
+            pout = np.empty(obound, np.uint8)
+            deflate.compress_pipelined(pin, sizes_u64, args.level, deflate.Format.Zlib, pout)
+            t0 = time.perf_counter()
+            _, _, psz2 = deflate.compress_pipelined(pin, sizes_u64, args.level, deflate.Format.Zlib, pout)
+            dtp = time.perf_counter() - t0
+            if psz2.tolist() != out_sizes:
+                raise SystemExit("pageable end-to-end sizes differ")
+            e2e["pageable"] = {"value": total / dtp / 1e9, "unit": UNIT, "ms_per_step": dtp * 1e3}
+            del pin, pout
+
+    # -- deflate_compress from 16 host threads at once (drop-in entry point)
+    threads16 = None
+    if world == 1 and not args.no_threads:
+        threads16 = measure_threads(deflate, buf, sizes, offs, args.level, 16, 1 << 30)
+
+    # -- the other configurations: whole-buffer text, pigz-style gzip and level-9 stress
+    configs = None
+    if world == 1 and not args.no_configs:
+        from orot_b200 import synth
+        nth = os.cpu_count() or 1
+        sm = clocks.get("sm_mhz")
+        configs = {}
+        text = synth.array(16 << 20, synth.TEXT, 42)
+        configs["text_16MiB_raw_L1_whole"] = measure_config(
+            deflate, "text", text, 1, 0, False, 0, stream, sh, 10, 16 << 20, 1, sm, sms)
+        mixed = synth.array(256 << 20, synth.MIXED, 7)
+        configs["mixed_256MiB_gzip_L6_parallel_128KiB"] = measure_config(
+            deflate, "mixed", mixed, 6, 2, True, 128 << 10, stream, sh, 3, 256 << 20, nth, sm, sms)
+        del mixed
+        for nm, kind, seed in (("random", synth.RANDOM, 99), ("periodic_1pct_flips", synth.PERIODIC, 98),
+                               ("text", synth.TEXT, 97)):
+            d = synth.array(1 << 30, kind, seed)
+            configs[f"stress_1GiB_{nm}_raw_L9_parallel_256KiB"] = measure_config(
+                deflate, nm, d, 9, 0, True, 256 << 10, stream, sh, 2, 64 << 20, nth, sm, sms)
+            del d
 
     # -- serving: Poisson arrivals through the continuous-batching server
     serving = None
     if args.serve_requests > 0 and world == 1:  # a one-GPU measurement; scaling runs skip it
-        serving = measure_serving(deflate, buf, total, args.serve_requests, args.serve_rate, seed=rank)
+        serving = measure_serving(deflate, buf, total, args.serve_requests, args.serve_rate,
+                                  args.serve_capacity_requests, seed=rank)
 
     # -- CPU baseline: the reference on the host cores (rank 0, N = 1 only)
     cpu = None
@@ -525,8 +839,8 @@ def main():
                        "format": "zlib", "graph": True, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}"},
             "ratio": ratio, "gpu_launches": launches_per_pass * args.steps, "e2e": e2e, "plain": plain,
-            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
-            "device_verify": device_verify,
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "threads16": threads16,
+            "configs": configs, "serving": serving, "device_verify": device_verify,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -26,6 +26,8 @@
 //   oracle_lz77                               token stream of one segment
 //   oracle_huffman_lengths                    code-length builder
 //   oracle_set_mode / oracle_limiter_events
+//   oracle_block_types                        block types of a raw stream (an
+//                                             RFC 1951 walker, test helper)
 
 #include <algorithm>
 #include <cstdint>
@@ -703,6 +705,141 @@ size_t oracle_parallel_compress(const void* in, size_t n, void* out, size_t cap,
     for (int i = 0; i < 4; ++i) dst[w++] = uint8_t(isz >> (8 * i));
   }
   return w;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- block walker
+// Not a restatement of the reference: an RFC 1951 reader that only walks a raw
+// DEFLATE stream's blocks (symbols are decoded and skipped, nothing is
+// written) and records each block's type.  The tests use it to say which
+// streams contain a stored block after a Huffman-coded block, the pattern the
+// reference's inflate misreads.
+namespace blockwalk {
+
+struct Reader {
+  const uint8_t* p;
+  size_t n, bit = 0;
+  bool bad = false;
+  uint32_t get(int k) {
+    uint32_t v = 0;
+    for (int i = 0; i < k; ++i, ++bit) {
+      if ((bit >> 3) >= n) { bad = true; return 0; }
+      v |= uint32_t((p[bit >> 3] >> (bit & 7)) & 1u) << i;
+    }
+    return v;
+  }
+};
+
+// Canonical code by counts per length and symbols in code order (RFC 1951
+// section 3.2.2): decoding reads one bit at a time and compares with the
+// first code of each length.
+struct Code {
+  int count[16] = {};
+  int sym[320] = {};
+  bool build(const uint8_t* len, int n) {
+    for (int i = 0; i < n; ++i) count[len[i]]++;
+    count[0] = 0;
+    int offs[16] = {}, left = 1;
+    for (int l = 1; l < 16; ++l) {
+      left = left * 2 - count[l];
+      if (left < 0) return false;
+      offs[l] = l == 1 ? 0 : offs[l - 1] + count[l - 1];
+    }
+    for (int i = 0; i < n; ++i)
+      if (len[i]) sym[offs[len[i]]++] = i;
+    return true;
+  }
+  int decode(Reader& r) const {
+    int code = 0, first = 0, index = 0;
+    for (int l = 1; l < 16; ++l) {
+      code |= int(r.get(1));
+      if (r.bad) return -1;
+      const int c = count[l];
+      if (code - first < c) return sym[index + code - first];
+      index += c;
+      first = (first + c) << 1;
+      code <<= 1;
+    }
+    return -1;
+  }
+};
+
+const int kLenExtra[29] = {0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5, 0};
+const int kDistExtra[30] = {0, 0, 0, 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13};
+
+bool skip_symbols(Reader& r, const Code& lit, const Code& dist) {
+  for (;;) {
+    const int s = lit.decode(r);
+    if (s < 0 || s > 285) return false;
+    if (s == 256) return true;
+    if (s > 256) {
+      r.get(kLenExtra[s - 257]);
+      const int d = dist.decode(r);
+      if (d < 0 || d > 29) return false;
+      r.get(kDistExtra[d]);
+      if (r.bad) return false;
+    }
+  }
+}
+
+}  // namespace blockwalk
+
+extern "C" {
+
+// Writes the type (0 stored, 1 fixed, 2 dynamic) of every block of the raw
+// DEFLATE stream p[0, n) into types[0, max); returns the number of blocks, or
+// -1 when the stream is malformed.
+long oracle_block_types(const void* data, size_t n, uint8_t* types, long max) {
+  using namespace blockwalk;
+  Reader r{static_cast<const uint8_t*>(data), n};
+  long nb = 0;
+  for (;;) {
+    const uint32_t last = r.get(1), type = r.get(2);
+    if (r.bad || type == 3) return -1;
+    if (nb < max) types[nb] = uint8_t(type);
+    ++nb;
+    if (type == 0) {
+      r.bit = (r.bit + 7) & ~size_t(7);
+      const uint32_t len = r.get(16), nlen = r.get(16);
+      if (r.bad || (len ^ 0xFFFFu) != nlen) return -1;
+      r.bit += size_t(len) * 8;
+      if ((r.bit >> 3) > n) return -1;
+    } else {
+      uint8_t lens[320] = {};
+      Code lit, dist;
+      if (type == 1) {
+        for (int i = 0; i < 288; ++i) lens[i] = i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : 8;
+        for (int i = 0; i < 30; ++i) lens[288 + i] = 5;
+        if (!lit.build(lens, 288) || !dist.build(lens + 288, 30)) return -1;
+      } else {
+        const int hlit = int(r.get(5)) + 257, hdist = int(r.get(5)) + 1, hclen = int(r.get(4)) + 4;
+        static const int order[19] = {16, 17, 18, 0, 8, 7, 9, 6, 10, 5, 11, 4, 12, 3, 13, 2, 14, 1, 15};
+        uint8_t cl[19] = {};
+        for (int i = 0; i < hclen; ++i) cl[order[i]] = uint8_t(r.get(3));
+        Code clc;
+        if (r.bad || !clc.build(cl, 19)) return -1;
+        int i = 0;
+        while (i < hlit + hdist) {
+          const int s = clc.decode(r);
+          if (s < 0) return -1;
+          if (s < 16) { lens[i++] = uint8_t(s); continue; }
+          int rep = 0, val = 0;
+          if (s == 16) { if (i == 0) return -1; val = lens[i - 1]; rep = 3 + int(r.get(2)); }
+          else if (s == 17) rep = 3 + int(r.get(3));
+          else rep = 11 + int(r.get(7));
+          if (r.bad || i + rep > hlit + hdist) return -1;
+          while (rep--) lens[i++] = uint8_t(val);
+        }
+        uint8_t ll[288] = {}, dl[32] = {};
+        std::memcpy(ll, lens, size_t(hlit));
+        std::memcpy(dl, lens + hlit, size_t(hdist));
+        if (!lit.build(ll, hlit) || !dist.build(dl, hdist)) return -1;
+      }
+      if (!skip_symbols(r, lit, dist)) return -1;
+    }
+    if (last) return nb;
+  }
 }
 
 }  // extern "C"

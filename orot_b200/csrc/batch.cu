@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <new>
 #include <vector>
 #include "engine_host.h"
 #include "../../include/orot_b200.h"
@@ -165,12 +167,28 @@ static bool batch_pack_to_host(deflate_gpu_batch* b, cudaStream_t st, void* host
   return true;
 }
 
+// The batch that the host-to-host batch calls reuse, one per device (that of
+// the calling thread), created on first use; callers hold global_mutex().
+static deflate_gpu_batch* host_batch() {
+  static deflate_gpu_batch* per_dev[kMaxDevices] = {};
+  const int dev = current_device();
+  if (dev < 0) return nullptr;
+  if (!per_dev[dev]) {
+    auto* b = new (std::nothrow) deflate_gpu_batch();
+    if (!b || !b->eng.ok) { delete b; return nullptr; }
+    per_dev[dev] = b;
+  }
+  return per_dev[dev];
+}
+
 extern "C" {
 
 deflate_gpu_batch* deflate_gpu_batch_new(void) {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); set_error("no CUDA device"); return nullptr; }
-  return new (std::nothrow) deflate_gpu_batch();
+  auto* b = new (std::nothrow) deflate_gpu_batch();
+  if (b && !b->eng.ok) { delete b; return nullptr; }
+  return b;
 }
 
 void deflate_gpu_batch_free(deflate_gpu_batch* b) { delete b; }
@@ -178,6 +196,7 @@ void deflate_gpu_batch_free(deflate_gpu_batch* b) { delete b; }
 int deflate_gpu_batch_load(deflate_gpu_batch* b, const void* concat, const size_t* sizes, size_t count, int level,
                            deflate_format format, int parallel, size_t block_size) {
   if (!b || (count && (!sizes || !concat)) || int(format) < 0 || int(format) > 2) return -1;
+  DeviceScope dev_scope(b->eng.device);
   std::vector<const void*> ptrs(count);
   const uint8_t* p = static_cast<const uint8_t*>(concat);
   for (size_t i = 0; i < count; ++i) { ptrs[i] = p; p += sizes[i]; }
@@ -188,6 +207,7 @@ int deflate_gpu_batch_load(deflate_gpu_batch* b, const void* concat, const size_
 
 int deflate_gpu_batch_run(deflate_gpu_batch* b, void* cuda_stream, int use_graph) {
   if (!b) return -1;
+  DeviceScope dev_scope(b->eng.device);
   Engine& e = b->eng;
   cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : e.stream;
   if (!use_graph) {
@@ -224,6 +244,7 @@ int deflate_gpu_batch_run(deflate_gpu_batch* b, void* cuda_stream, int use_graph
 
 int deflate_gpu_batch_sizes(deflate_gpu_batch* b, size_t* out_sizes) {
   if (!b || !b->ran) return -1;
+  DeviceScope dev_scope(b->eng.device);
   Engine& e = b->eng;
   if (cudaDeviceSynchronize() != cudaSuccess) { set_error(cudaGetErrorString(cudaGetLastError())); return -1; }
   std::vector<Stream> s(e.streams.size());
@@ -238,6 +259,7 @@ int deflate_gpu_batch_sizes(deflate_gpu_batch* b, size_t* out_sizes) {
 
 int deflate_gpu_batch_verify(deflate_gpu_batch* b, int* ok) {
   if (!b || !b->ran || !ok) return -1;
+  DeviceScope dev_scope(b->eng.device);
   Engine& e = b->eng;
   if (cudaDeviceSynchronize() != cudaSuccess) { set_error(cudaGetErrorString(cudaGetLastError())); return -1; }
   const size_t n = e.streams.size();
@@ -309,6 +331,7 @@ int deflate_gpu_batch_verify(deflate_gpu_batch* b, int* ok) {
 
 size_t deflate_gpu_batch_output(deflate_gpu_batch* b, size_t i, void* dst, size_t cap) {
   if (!b || !b->ran || i >= b->eng.streams.size()) return 0;
+  DeviceScope dev_scope(b->eng.device);
   Engine& e = b->eng;
   Stream s{};
   if (cudaDeviceSynchronize() != cudaSuccess ||
@@ -329,6 +352,7 @@ int deflate_gpu_batch_launches(const deflate_gpu_batch* b) { return b ? b->launc
 
 int deflate_gpu_batch_profile(deflate_gpu_batch* b, int enable) {
   if (!b) return -1;
+  DeviceScope dev_scope(b->eng.device);
   b->eng.marks.on = enable != 0;
   drop_graph(b);  // a captured graph carries no event records
   return 0;
@@ -336,6 +360,7 @@ int deflate_gpu_batch_profile(deflate_gpu_batch* b, int enable) {
 
 int deflate_gpu_batch_phase_ms(deflate_gpu_batch* b, float* ms, int max) {
   if (!b || !ms || max < int(kNumPhases)) return -1;
+  DeviceScope dev_scope(b->eng.device);
   if (cudaDeviceSynchronize() != cudaSuccess) return -1;
   b->eng.phase_ms(ms);
   return int(kNumPhases);
@@ -352,8 +377,8 @@ size_t deflate_gpu_compress_batch(const void* const* in, const size_t* in_sizes,
   if (!count) return 0;
   if (!in || !in_sizes || !out || !out_caps || !out_sizes || int(format) < 0 || int(format) > 2) return 0;
   std::lock_guard<std::mutex> lk(global_mutex());
-  static deflate_gpu_batch* gb = new deflate_gpu_batch();
-  deflate_gpu_batch* b = gb;
+  deflate_gpu_batch* b = host_batch();
+  if (!b) return 0;
   Engine& e = b->eng;
   if (!batch_setup(b, in, nullptr, in_sizes, count, level, int(format), false, 0, e.stream)) return 0;
   if (!e.launch(e.stream)) return 0;
@@ -385,8 +410,8 @@ size_t deflate_gpu_compress_packed(const void* in_concat, const size_t* in_sizes
   for (size_t i = 0; i < count; ++i) total_in += in_sizes[i];
   if (total_in && !in_concat) return 0;
   std::lock_guard<std::mutex> lk(global_mutex());
-  static deflate_gpu_batch* gb = new deflate_gpu_batch();
-  deflate_gpu_batch* b = gb;
+  deflate_gpu_batch* b = host_batch();
+  if (!b) return 0;
   Engine& e = b->eng;
   if (!batch_setup(b, nullptr, static_cast<const uint8_t*>(in_concat), in_sizes, count, level, int(format), false, 0,
                    e.stream))

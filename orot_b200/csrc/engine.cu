@@ -13,7 +13,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 #include "engine.cuh"
@@ -73,10 +75,13 @@ bool HostBuf::ensure(size_t n) {
 void HostBuf::release() { if (p) cudaFreeHost(p); p = nullptr; cap = 0; }
 
 Engine::Engine() {
-  cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
-  upload_crc_tables();
+  ok = cudaGetDevice(&device) == cudaSuccess &&
+       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+       cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) == cudaSuccess && upload_crc_tables();
+  if (!ok) {
+    cudaGetLastError();
+    set_error("engine set-up failed (no usable CUDA device)");
+  }
   // Tile size override (bytes, multiple of 32, at most 64 KiB) for tests.
   if (const char* v = std::getenv("OROT_B200_TILE")) {
     const long t = std::strtol(v, nullptr, 10);
@@ -96,17 +101,21 @@ Engine::~Engine() {
   if (stream) cudaStreamDestroy(stream);
 }
 
-// Tile size: 64 KiB, halved (down to 16 KiB) while the pass would have fewer
-// than 64 tiles per SM.  One warp walks a 64 KiB tile in ~3 ms, and a pass
+// Tile size: 64 KiB, halved while the pass would have fewer than 64 tiles per
+// SM, down to 8 KiB at 12 hash bits and 16 KiB at 14 (a tile carries in a
+// head table of 4 B per entry, 16 KB and 64 KB, so smaller tiles would move
+// more table than input).  One warp walks a 64 KiB tile in ~3 ms, and a pass
 // ends about one tile time after its last tiles start: a pass of a few
 // hundred MiB (a pipelined group, a served batch) finishes sooner with
-// smaller tiles (+6% host-to-host on 512 MiB groups with 32 KiB tiles),
-// while a pass of gigabytes keeps 64 KiB tiles, whose fix-up and carried
-// tables cost less (-3% at 32 KiB on the 5 GB batch).
-uint32_t Engine::pick_tile(uint64_t total_bytes) const {
+// smaller tiles (+6% host-to-host on 512 MiB groups with 32 KiB tiles), a
+// single call of a few hundred KiB is walked by more warps at once, while a
+// pass of gigabytes keeps 64 KiB tiles, whose fix-up and carried tables cost
+// less (-3% at 32 KiB on the 5 GB batch).
+uint32_t Engine::pick_tile(uint64_t total_bytes, int hash_bits) const {
   uint32_t t = 65536;
+  const uint32_t tmin = hash_bits <= 12 ? 8192 : 16384;
   const uint64_t want = uint64_t(sms) * 64;
-  while (t > 16384 && (total_bytes + t - 1) / t < want) t >>= 1;
+  while (t > tmin && (total_bytes + t - 1) / t < want) t >>= 1;
   if (tile_override) t = tile_override;
   return t;
 }
@@ -124,7 +133,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
   for (auto& l : lists) l.clear();
   uint64_t total = 0;
   for (const Job& j : jobs) total += j.in_len;
-  const uint32_t T = pick_tile(total);
+  const uint32_t T12 = pick_tile(total, 12), T14 = pick_tile(total, 14);
   uint64_t scratch = 0;
   uint32_t npieces = 0;
   for (size_t ji = 0; ji < jobs.size(); ++ji) {
@@ -157,6 +166,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
       const int hb = lv <= 0 ? 0 : lv == 1 ? 12 : lv <= 3 ? 14 : 0;
       const uint32_t H = hb ? (1u << hb) : 0;
       if (lv > 0 && lv <= 3) {
+        const uint32_t T = hb == 12 ? T12 : T14;
         const uint32_t nt = len ? uint32_t((len + T - 1) / T) : 1;
         g.tile_count = nt;
         const uint32_t seg_index = uint32_t(segs.size());
@@ -243,6 +253,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
     std::vector<uint32_t>& v = lists[li];
     std::vector<uint32_t> part;
     size_t nfull = 0;
+    const uint32_t T = li == kWalk12 ? T12 : T14;
     for (const uint32_t x : v) {
       if (tiles[x].len == T) v[nfull++] = x;
       else part.push_back(x);
@@ -472,7 +483,67 @@ uint32_t Engine::checksum_device(uint32_t init, const uint8_t* d_data, size_t n,
 
 std::mutex& global_mutex() { static std::mutex m; return m; }
 deflate_allocator g_allocator{};  // set by deflate_set_allocator, never used to allocate
-Engine& global_engine() { static Engine* e = new Engine(); return *e; }
+
+int current_device() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return -1;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("CUDA device index above 63");
+    return -1;
+  }
+  return dev;
+}
+
+namespace {
+struct EnginePool {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Engine*> idle;  // most recently returned last
+  int created = 0;
+};
+EnginePool& pool_of(int dev) {
+  static EnginePool pools[kMaxDevices];
+  return pools[dev];
+}
+}  // namespace
+
+EngineLease::EngineLease() {
+  dev_ = current_device();
+  if (dev_ < 0) return;
+  EnginePool& P = pool_of(dev_);
+  std::unique_lock<std::mutex> lk(P.mu);
+  P.cv.wait(lk, [&] { return !P.idle.empty() || P.created < kMaxEngines; });
+  if (!P.idle.empty()) {
+    e_ = P.idle.back();
+    P.idle.pop_back();
+    return;
+  }
+  ++P.created;
+  lk.unlock();
+  Engine* e = new (std::nothrow) Engine();  // binds to this thread's current device, dev_
+  if (e && e->ok) {
+    e_ = e;
+    return;
+  }
+  delete e;
+  lk.lock();
+  --P.created;
+  P.cv.notify_one();
+}
+
+EngineLease::~EngineLease() {
+  if (!e_) return;
+  EnginePool& P = pool_of(dev_);
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    P.idle.push_back(e_);
+  }
+  P.cv.notify_one();
+}
 
 }  // namespace orotb
 
@@ -502,8 +573,8 @@ size_t deflate_compress(const void* in, size_t n, void* out, size_t cap, int lev
   if (fmt < 0 || fmt > 2) return 0;
   if (cap < framed_bound(n, fmt)) return 0;
   if ((n && !in) || !out) return 0;
-  std::lock_guard<std::mutex> lk(global_mutex());
-  return global_engine().compress_host(in, n, out, cap, level, fmt, false, 0);
+  EngineLease e;
+  return e ? e->compress_host(in, n, out, cap, level, fmt, false, 0) : 0;
 }
 
 deflate_parallel_ctx* deflate_parallel_new(int level, deflate_format f, int, size_t block) {
@@ -514,19 +585,19 @@ void deflate_parallel_free(deflate_parallel_ctx* c) { delete c; }
 
 size_t deflate_parallel_compress(deflate_parallel_ctx* c, const void* in, size_t n, void* out, size_t cap) {
   if (!c || (n && !in) || !out) return 0;
-  std::lock_guard<std::mutex> lk(global_mutex());
-  return global_engine().compress_host(in, n, out, cap, c->level, c->fmt, true, c->block);
+  EngineLease e;
+  return e ? e->compress_host(in, n, out, cap, c->level, c->fmt, true, c->block) : 0;
 }
 
 uint32_t deflate_crc32(uint32_t init, const void* data, size_t len) {
   if (!data || !len) return init;
-  std::lock_guard<std::mutex> lk(global_mutex());
-  return global_engine().checksum_host(init, data, len, false);
+  EngineLease e;
+  return e ? e->checksum_host(init, data, len, false) : init;
 }
 uint32_t deflate_adler32(uint32_t init, const void* data, size_t len) {
   if (!data || !len) return init;
-  std::lock_guard<std::mutex> lk(global_mutex());
-  return global_engine().checksum_host(init, data, len, true);
+  EngineLease e;
+  return e ? e->checksum_host(init, data, len, true) : init;
 }
 
 const char* orot_b200_last_error(void) { return g_err.c_str(); }

@@ -70,9 +70,10 @@ class Engine {
   // Checksum of n bytes already on the device (d_data 16-byte aligned, with
   // readable padding after the last byte).
   uint32_t checksum_device(uint32_t init, const uint8_t* d_data, size_t n, bool adler);
-  uint32_t pick_tile(uint64_t total_bytes) const;
+  uint32_t pick_tile(uint64_t total_bytes, int hash_bits) const;
 
   int device = 0, sms = 148;
+  bool ok = false;  // the stream and the device's constant tables are set up
   cudaStream_t stream = nullptr;
   DevBuf d_in, d_out, d_scratch, d_tables, d_pack;
   HostBuf h_tables, h_stage;
@@ -97,7 +98,55 @@ class Engine {
 };
 
 std::mutex& global_mutex();
-Engine& global_engine();
+
+// The one-call entry points (deflate_compress, deflate_parallel_compress,
+// deflate_crc32/adler32, deflate_decompress, the shard call) run on engines
+// of the calling thread's current CUDA device.  A lease takes an idle engine
+// of that device, creating one when none is idle (at most kMaxEngines per
+// device; beyond that the caller waits for one), so calls from different
+// host threads run at the same time, each on its own stream and arenas.
+// Engines are kept for reuse, most recently used first, so a single-threaded
+// caller keeps reusing one engine and its grown arenas.
+constexpr int kMaxEngines = 32;
+constexpr int kMaxDevices = 64;
+class EngineLease {
+ public:
+  EngineLease();
+  ~EngineLease();
+  EngineLease(const EngineLease&) = delete;
+  EngineLease& operator=(const EngineLease&) = delete;
+  explicit operator bool() const { return e_ != nullptr; }
+  Engine& operator*() const { return *e_; }
+  Engine* operator->() const { return e_; }
+
+ private:
+  Engine* e_ = nullptr;
+  int dev_ = -1;
+};
+
+// Makes `dev` the calling thread's current device for the scope and restores
+// the caller's device afterwards: objects bound to a device (a batch, a lane)
+// may be used from threads whose current device is another one.
+class DeviceScope {
+ public:
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != dev) changed_ = cudaSetDevice(dev) == cudaSuccess;
+    cudaGetLastError();
+  }
+  ~DeviceScope() {
+    if (changed_) cudaSetDevice(prev_);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+
+ private:
+  int prev_ = -1;
+  bool changed_ = false;
+};
+
+// The calling thread's current device, or -1 (with the error recorded) when
+// it has none or its index is beyond kMaxDevices.
+int current_device();
 
 // Packs every stream's output of the last pass at 16-byte aligned offsets
 // (d_off: count + 1 entries, the last the total) and optionally writes the

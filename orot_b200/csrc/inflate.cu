@@ -10,6 +10,7 @@
 // return DEFLATE_DATA_ERROR, as in the reference.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <numeric>
@@ -93,6 +94,11 @@ static bool decode_raw(Engine& e, const uint8_t* raw, size_t len, size_t out_off
   return true;
 }
 
+// Most bytes n bytes of DEFLATE data can decode to: the densest token is a
+// 258-byte match coded in 2 bits (1-bit length and distance codes, no extra
+// bits), 1032 bytes per input byte; stored blocks expand less.
+static size_t max_inflated(size_t n) { return n > (SIZE_MAX - 64) / 1032 ? SIZE_MAX - 64 : n * 1032 + 64; }
+
 static uint32_t le32(const uint8_t* t) {
   return uint32_t(t[0]) | (uint32_t(t[1]) << 8) | (uint32_t(t[2]) << 16) | (uint32_t(t[3]) << 24);
 }
@@ -102,6 +108,7 @@ static uint32_t le32(const uint8_t* t) {
 // to contain a header-like byte pattern that the parallel path splits on.
 static deflate_result gzip_members_sequential(Engine& e, const uint8_t* in, size_t n, uint8_t* out, size_t cap,
                                               size_t* actual) {
+  cap = std::min(cap, max_inflated(n));
   if (!e.ensure_io(align_up(n, 16) + 64, align_up(cap, 16) + 64)) return DEFLATE_MEM_ERROR;
   size_t pos = 0, total = 0;
   while (pos < n) {
@@ -152,9 +159,12 @@ static deflate_result decompress_one(Engine& e, const uint8_t* in, size_t n, uin
   size_t off = 0, rlen = 0;
   const deflate_result fr = frame_range(in, n, fmt, &off, &rlen);
   if (fr != DEFLATE_OK) return fr;
-  if (!e.ensure_io(align_up(rlen, 16) + 64, align_up(cap, 16) + 64)) return DEFLATE_MEM_ERROR;
+  // The device arena holds at most what rlen bytes can expand to (not the
+  // caller's whole capacity, which may exceed free device memory).
+  const size_t dcap = std::min(cap, max_inflated(rlen));
+  if (!e.ensure_io(align_up(rlen, 16) + 64, align_up(dcap, 16) + 64)) return DEFLATE_MEM_ERROR;
   InflateJob job;
-  if (!decode_raw(e, in + off, rlen, 0, cap, &job)) return DEFLATE_MEM_ERROR;
+  if (!decode_raw(e, in + off, rlen, 0, dcap, &job)) return DEFLATE_MEM_ERROR;
   bool good = job.status == kInfOk;
   const uint8_t* t = in + n;  // trailer
   if (good && fmt == int(DEFLATE_FORMAT_ZLIB)) {
@@ -186,7 +196,8 @@ extern "C" deflate_result deflate_decompress(const void* in, size_t in_size, voi
                                              size_t* actual_out_size, deflate_format format) {
   const int fmt = int(format);
   if (fmt < 0 || fmt > 2 || (in_size && !in) || (out_capacity && !out)) return DEFLATE_PARAM_ERROR;
-  std::lock_guard<std::mutex> lk(global_mutex());
-  return decompress_host(global_engine(), static_cast<const uint8_t*>(in), in_size, static_cast<uint8_t*>(out),
+  EngineLease e;
+  if (!e) return DEFLATE_MEM_ERROR;
+  return decompress_host(*e, static_cast<const uint8_t*>(in), in_size, static_cast<uint8_t*>(out),
                          out_capacity, actual_out_size, fmt);
 }

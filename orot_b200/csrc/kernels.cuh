@@ -67,7 +67,7 @@ void launch_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total, uint32_t 
 CrcPowers host_crc_powers();
 void launch_join(const Work& wk, uint32_t* counter, cudaStream_t st, int sms);
 void launch_frame(const Work& wk, cudaStream_t st);
-void upload_crc_tables();
+bool upload_crc_tables();  // once per device; false on a device error
 
 // One DEFLATE stream to decode (raw data, framing stripped by the host).
 struct InflateJob {

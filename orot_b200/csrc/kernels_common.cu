@@ -14,6 +14,7 @@
 //               inside a copy, atomicOr on the two boundary words it shares.
 //   k_frame     zlib / gzip header and trailer bytes.
 #include <cuda_runtime.h>
+#include <mutex>
 #include <cstdint>
 #include "engine.cuh"
 #include "deflate_device.cuh"
@@ -353,9 +354,16 @@ __global__ void k_frame(Work wk) {
 }
 
 // ---------------------------------------------------------------- launchers
-void upload_crc_tables() {
-  static bool done = false;
-  if (done) return;
+// The constant tables live in each device's own constant memory, so they are
+// uploaded once per device (under a lock: engines of one device may be
+// created by several host threads at once).
+bool upload_crc_tables() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return true;
   uint32_t t[4][256];
   for (uint32_t i = 0; i < 256; ++i) {
     uint32_t c = i;
@@ -364,14 +372,18 @@ void upload_crc_tables() {
   }
   for (int s = 1; s < 4; ++s)
     for (int i = 0; i < 256; ++i) t[s][i] = (t[s - 1][i] >> 8) ^ t[0][t[s - 1][i] & 0xFF];
-  cudaMemcpyToSymbol(c_crc_slice, t, sizeof t);
   CrcPowers pw = host_crc_powers();
   uint32_t sub[9];
   for (int s = 0; s < 9; ++s) sub[s] = xpow8n(pw, uint64_t(kCkSub) << s);
-  cudaMemcpyToSymbol(c_crc_sub, sub, sizeof sub);
   const uint32_t blk = xpow8n(pw, kCkBlock);
-  cudaMemcpyToSymbol(c_crc_block, &blk, sizeof blk);
-  done = true;
+  if (cudaMemcpyToSymbol(c_crc_slice, t, sizeof t) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_crc_sub, sub, sizeof sub) != cudaSuccess ||
+      cudaMemcpyToSymbol(c_crc_block, &blk, sizeof blk) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  done[dev] = true;
+  return true;
 }
 
 CrcPowers host_crc_powers() {

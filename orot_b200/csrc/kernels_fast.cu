@@ -544,11 +544,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_fix2(Work wk, const uint32_t* __
   const uint32_t si = blockIdx.x * WARPS + wid;
   if (si >= nseg) return;
   const Segment sg = wk.segs[seglist[si]];
+  const uint32_t lane = threadIdx.x & 31;
   uint32_t exit = wk.tiles[sg.tile_first].fin_exit;
-  for (uint32_t k = 1; k < sg.tile_count; ++k) {
-    Tile* tp = wk.tiles + sg.tile_first + k;
-    if (tp->fix_entry == exit) { exit = tp->fin_exit; continue; }
-    exit = fix_apply(wk, tp, exit, sm[wid], sm[wid] + kRing);
+  // The entries and exits of 32 tiles are loaded at once (one memory latency
+  // instead of one per tile) and followed through shuffles; fix_apply changes
+  // only its own tile, so the loaded values of the later tiles stay valid.
+  for (uint32_t k0 = 1; k0 < sg.tile_count; k0 += 32) {
+    const uint32_t cnt = min(32u, sg.tile_count - k0);
+    uint32_t ent = 0, ext = 0;
+    if (lane < cnt) {
+      const Tile* t = wk.tiles + sg.tile_first + k0 + lane;
+      ent = t->fix_entry;
+      ext = t->fin_exit;
+    }
+    for (uint32_t j = 0; j < cnt; ++j) {
+      const uint32_t ej = __shfl_sync(kFull, ent, j);
+      const uint32_t xj = __shfl_sync(kFull, ext, j);
+      if (ej == exit) { exit = xj; continue; }
+      exit = fix_apply(wk, wk.tiles + sg.tile_first + k0 + j, exit, sm[wid], sm[wid] + kRing);
+    }
   }
 }
 
@@ -774,7 +788,10 @@ static uint32_t* noalloc_scratch_ptr(int dev) {
   static std::mutex mu;
   static uint32_t* ptrs[64] = {};
   static bool init[64] = {};
-  if (dev < 0 || dev >= 64) return nullptr;
+  if (dev < 0 || dev >= 64) {
+    set_error("deflate_gpu_compress_noalloc: CUDA device index above 63");
+    return nullptr;
+  }
   std::lock_guard<std::mutex> lk(mu);
   if (!init[dev]) {
     void* p = nullptr;
@@ -829,7 +846,12 @@ extern "C" int deflate_gpu_compress_noalloc(const void* d_in, size_t in_size, vo
     k_noalloc<12><<<1, 256, smem, st>>>(in, n, out, level, lv, fmt, scratch, d_out_size);
   } else {
     const size_t smem = size_t(walker_words<14>()) * 4;
-    cudaFuncSetAttribute(k_noalloc<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const cudaError_t a = cudaFuncSetAttribute(k_noalloc<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (a != cudaSuccess) {
+      cudaGetLastError();
+      set_error(std::string("deflate_gpu_compress_noalloc shared-memory set-up: ") + cudaGetErrorString(a));
+      return -6;
+    }
     k_noalloc<14><<<1, 256, smem, st>>>(in, n, out, level, lv, fmt, scratch, d_out_size);
   }
   const cudaError_t e = cudaGetLastError();

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -501,9 +502,17 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
                                       uint64_t* out_offsets, size_t* out_sizes, size_t group_bytes, int lanes) {
   if (!count || !in_sizes || !out_packed || !out_offsets || !out_sizes || int(format) < 0 || int(format) > 2) return 0;
   std::lock_guard<std::mutex> lk(global_mutex());
-  static std::vector<Lane*> pool;
+  // lanes are kept per device (the calling thread's) and reused across calls
+  static std::vector<Lane*> pools[kMaxDevices];
+  const int dev = current_device();
+  if (dev < 0) return 0;
+  std::vector<Lane*>& pool = pools[dev];
   const int nl = lanes > 0 ? std::min(lanes, 8) : 4;
-  while (int(pool.size()) < nl) pool.push_back(new Lane());
+  while (int(pool.size()) < nl) {
+    Lane* L = new (std::nothrow) Lane();
+    if (!L || !L->eng.ok) { delete L; set_error("lane set-up failed"); return 0; }
+    pool.push_back(L);
+  }
   if (!group_bytes) group_bytes = size_t(512) << 20;
   // groups: contiguous buffer ranges
   std::vector<size_t> gfirst, gcount;

@@ -30,10 +30,11 @@ int deflate_gpu_parallel_shard(const void* in, size_t in_size, int level, deflat
   *out_size = 0;
   *checksum = fmt == int(DEFLATE_FORMAT_ZLIB) ? 1u : 0u;  // checksums of an empty range
   if (in_size == 0 && !final_part) return 0;             // a rank without chunks adds nothing
-  std::lock_guard<std::mutex> lk(global_mutex());
+  EngineLease e;
+  if (!e) return -2;
   Stream s{};
   const uint32_t mode = kStreamBare | (final_part ? 0u : kStreamOpen);
-  const size_t r = global_engine().compress_host(in, in_size, out, out_capacity, level, fmt, true, block_size, mode, &s);
+  const size_t r = e->compress_host(in, in_size, out, out_capacity, level, fmt, true, block_size, mode, &s);
   if (r == 0) return s.error == kErrCapacity || s.out_size > out_capacity ? -3 : -2;
   *out_size = r;
   if (fmt != int(DEFLATE_FORMAT_RAW)) *checksum = s.checksum;

@@ -52,6 +52,8 @@ class Oracle:
         L.oracle_huffman_lengths.argtypes = [c.c_void_p, c.c_int, c.c_void_p, c.c_int]
         L.oracle_set_mode.argtypes = [c.c_int]
         L.oracle_limiter_events.restype = c.c_long
+        L.oracle_block_types.restype = c.c_long
+        L.oracle_block_types.argtypes = [c.c_void_p, c.c_size_t, c.c_void_p, c.c_long]
         self.L = L
 
     def compress(self, data: bytes, level: int, fmt: int) -> bytes:
@@ -73,6 +75,19 @@ class Oracle:
 
     def adler32(self, data: bytes, init: int = 1) -> int:
         return self.L.oracle_adler32(init, data, len(data))
+
+    def block_types(self, raw: bytes) -> list:
+        """Types (0 stored, 1 fixed, 2 dynamic) of the blocks of a raw
+        DEFLATE stream; raises on a malformed stream."""
+        cap = 1 << 16
+        while True:
+            t = ctypes.create_string_buffer(cap)
+            k = self.L.oracle_block_types(raw, len(raw), t, cap)
+            if k < 0:
+                raise ValueError("malformed DEFLATE stream")
+            if k <= cap:
+                return list(t.raw[:k])
+            cap = k
 
     def tokens(self, data: bytes, level: int):
         import numpy as np

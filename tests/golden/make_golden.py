@@ -1,8 +1,9 @@
 """Generates tests/golden/reference_vectors.json from the reference itself.
 
-Run in a checkout that has the daramkun/orot sources at /root/reference:
+Run where the daramkun/orot sources are, after building the reference from
+them (REF names the source tree):
 
-    make -f oracle/Makefile.ref          # builds oracle/_ref/liborot_ref.so
+    make -f oracle/Makefile.ref REF=<reference tree>   # oracle/_ref/liborot_ref.so
     python tests/golden/make_golden.py
 
 For every case (input kind/size/seed from orot_b200.synth, level, format,

@@ -147,3 +147,22 @@ def test_more_host_side_rejections(lib):
                                             c.c_double]
     assert lib.deflate_gpu_server_submit(None, b"abc", 3, out, 64, 1, 0) == 0
     assert lib.deflate_gpu_server_wait(None, 1, None, None, 0.0) == -1
+
+
+def test_reference_unit_tests_link_the_engine():
+    """The reference's unit tests (built by oracle/Makefile.ref) resolve their
+    deflate_* calls to liborot_b200.so, not to the reference's archive linked
+    after it (no execution here: that is a GPU test)."""
+    import subprocess
+    unit = os.path.join(ROOT, "oracle", "_ref", "unit")
+    if not os.path.isdir(unit):
+        pytest.skip("reference unit tests not built on this machine")
+    for name in ["test_deflate_roundtrip", "test_deflate_levels", "test_deflate_formats", "test_deflate_simd",
+                 "test_deflate_parallel"]:
+        exe = os.path.join(unit, name)
+        undefined = subprocess.run(["nm", "-u", exe], capture_output=True, text=True).stdout
+        defined = subprocess.run(["nm", "--defined-only", exe], capture_output=True, text=True).stdout
+        assert " deflate_" not in defined, name          # nothing taken from the archive
+        assert "deflate_compress" in undefined or "deflate_crc32" in undefined or "deflate_parallel" in undefined
+        ldd = subprocess.run(["ldd", exe], capture_output=True, text=True).stdout
+        assert "liborot_b200.so" in ldd and "not found" not in ldd.split("liborot_b200.so")[1].split("\n")[0]

@@ -21,3 +21,15 @@ def test_small_crafted_stream():
     raw, data = crafted_stream(7, tokens=120)
     assert zlib.decompress(raw, -15) == data
     assert 300 < len(raw) < 4000
+
+
+def test_block_walker_reads_block_types(oracle):
+    """The oracle's block walker (used to explain the reference inflate's
+    failures) reports the planned block types of the crafted streams, and
+    zlib's own single dynamic block."""
+    for seed in range(3):
+        raw, _ = crafted_stream(seed, tokens=800)
+        assert oracle.block_types(raw) == [2, 1, 0, 2, 2, 0, 2, 1]
+    d = bytes(range(256)) * 300
+    assert oracle.block_types(zlib.compress(d, 9)[2:-4]) == [2]
+    assert oracle.block_types(zlib.compress(b"", 0)[2:-4]) in ([1], [0])

@@ -42,6 +42,33 @@ def test_server_alone_equals_mix(gpu):
     srv.close()
 
 
+def test_server_large_requests_alone_equal_mix(gpu):
+    """The serving workload's largest class (4-16 MiB, levels 1 and 6) mixed
+    with small requests and submitted while earlier passes run: each result
+    equals its single deflate_compress call byte for byte."""
+    rng = random.Random(5)
+    reqs = []
+    for i in range(36):
+        if i % 3 == 0:
+            n = int(np.exp(rng.uniform(np.log(4 << 20), np.log(16 << 20))))
+        else:
+            n = int(np.exp(rng.uniform(np.log(4 << 10), np.log(4 << 20))))
+        reqs.append((synth.gen(n, synth.MIXED if i % 2 else rng.randint(0, 5), 500 + i), rng.choice([1, 1, 6]), 0))
+    singles = [gpu.compress(d, lv, gpu.Format(f)) for d, lv, f in reqs]
+    srv = gpu.Server(device_budget=16 << 30, lanes=3)
+    tickets = []
+    for k, (d, lv, f) in enumerate(reqs):
+        tickets.append(srv.submit(d, lv, gpu.Format(f)))
+        if k % 6 == 5:
+            time.sleep(0.01)  # later requests arrive while earlier passes run
+    for t, ref in zip(tickets, singles):
+        out, _ = srv.wait(t, timeout=300)
+        assert out == ref
+    passes, _ = srv.stats()
+    assert passes >= 2
+    srv.close()
+
+
 def test_server_poisoned_request_fails_alone(gpu):
     reqs = _requests(12, 2, max_size=1 << 20)
     srv = gpu.Server(lanes=2)
