@@ -837,7 +837,7 @@ def main():
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": WORKLOAD, "buffers": args.buffers, "bytes_per_gpu": total, "level": args.level,
                        "format": "zlib", "graph": True, "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "geometry": deflate.geometry_source()},
             "ratio": ratio, "gpu_launches": launches_per_pass * args.steps, "e2e": e2e, "plain": plain,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks, "threads16": threads16,
             "configs": configs, "serving": serving, "device_verify": device_verify,

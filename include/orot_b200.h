@@ -284,6 +284,11 @@ int deflate_gpu_compress_noalloc(const void* d_in, size_t in_size, void* d_out, 
 /* Last error message of the calling thread ("" if none). */
 const char* orot_b200_last_error(void);
 
+/* Where the pass geometry (tile bytes, lazy-level run lengths per pass size)
+ * compiled into this library came from: the autotuner's device and date, or
+ * the hand-set rules it starts from (no counterpart in the reference). */
+const char* orot_b200_geometry_source(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,7 @@
 #include "engine.cuh"
 #include "kernels.cuh"
 #include "engine_host.h"
+#include "geometry_table.h"
 #include "../../include/orot_b200.h"
 
 namespace orotb {
@@ -101,23 +102,24 @@ Engine::~Engine() {
   if (stream) cudaStreamDestroy(stream);
 }
 
-// Tile size: 64 KiB, halved while the pass would have fewer than 64 tiles per
-// SM, down to 8 KiB at 12 hash bits and 16 KiB at 14 (a tile carries in a
-// head table of 4 B per entry, 16 KB and 64 KB, so smaller tiles would move
-// more table than input).  One warp walks a 64 KiB tile in ~3 ms, and a pass
-// ends about one tile time after its last tiles start: a pass of a few
-// hundred MiB (a pipelined group, a served batch) finishes sooner with
-// smaller tiles (+6% host-to-host on 512 MiB groups with 32 KiB tiles), a
-// single call of a few hundred KiB is walked by more warps at once, while a
-// pass of gigabytes keeps 64 KiB tiles, whose fix-up and carried tables cost
-// less (-3% at 32 KiB on the 5 GB batch).
+// Pass geometry comes from the table the autotuner writes (geometry_table.h):
+// the row of the largest pass-size class the pass reaches.  Classes are
+// measured on 148 SMs; a device with fewer SMs reaches the same work per SM
+// with proportionally less input.  Small tiles let more warps walk a small
+// pass at once; large tiles carry fewer head tables (4 B per entry: 16 KB
+// at 12 hash bits, 64 KB at 14) and fix up fewer boundaries.
+const GeometryRow& Engine::geometry(uint64_t total_bytes) const {
+  const uint64_t scaled = total_bytes / uint64_t(std::max(sms, 1)) * 148u;
+  size_t k = 0;
+  for (size_t i = 0; i < sizeof(kGeometry) / sizeof(kGeometry[0]); ++i)
+    if (scaled >= kGeometry[i].min_bytes) k = i;
+  return kGeometry[k];
+}
+
 uint32_t Engine::pick_tile(uint64_t total_bytes, int hash_bits) const {
-  uint32_t t = 65536;
-  const uint32_t tmin = hash_bits <= 12 ? 8192 : 16384;
-  const uint64_t want = uint64_t(sms) * 64;
-  while (t > tmin && (total_bytes + t - 1) / t < want) t >>= 1;
-  if (tile_override) t = tile_override;
-  return t;
+  if (tile_override) return tile_override;
+  const GeometryRow& g = geometry(total_bytes);
+  return hash_bits <= 12 ? g.tile12 : g.tile14;
 }
 
 template <class T>
@@ -272,18 +274,15 @@ bool Engine::plan(const std::vector<Job>& jobs) {
   off_ck = put_table(buf, cks);
   // Lazy tiles go to CTAs in runs of consecutive tiles of one segment (the
   // window slides from tile to tile, and every run first builds the links of
-  // its whole window); runs shorten when there are too few tiles to give
-  // every SM several, and keep ~20 runs per SM (one CTA per SM) down to 16
-  // tiles, so that the last wave of runs is a small part of a pass: a 203 MB
-  // pass at level 6 runs 3% faster with runs of 16 than of 32, a 5.1 GB pass
-  // 4% slower.
+  // its whole window).  Short runs give small passes enough CTAs for every
+  // SM; long runs build fewer windows.  The run length per level group and
+  // pass size is the autotuner's (geometry_table.h).
   if (!lists[kLazySegs].empty()) {
-    const uint32_t n = uint32_t(lists[kLazyTiles].size());
-    const uint32_t by_sm = std::max(1u, std::min(kLazyRun, n / (4u * uint32_t(sms))));
-    const uint32_t R = lazy_run_override ? lazy_run_override
-                                         : std::min(by_sm, std::max(16u, n / (20u * uint32_t(sms))));
+    const GeometryRow& geo = geometry(total);
     for (uint32_t si : lists[kLazySegs]) {
       const Segment& g = segs[si];
+      const int grp = g.level <= 6 ? 0 : g.level <= 9 ? 1 : 2;
+      const uint32_t R = std::min(kLazyRun, std::max(1u, lazy_run_override ? lazy_run_override : geo.lazy_run[grp]));
       for (uint32_t t = 0; t < g.tile_count; t += R) {
         lists[kLazyRuns].push_back(g.tile_first + t);
         lists[kLazyRuns].push_back(std::min(R, g.tile_count - t));
@@ -601,5 +600,6 @@ uint32_t deflate_adler32(uint32_t init, const void* data, size_t len) {
 }
 
 const char* orot_b200_last_error(void) { return g_err.c_str(); }
+const char* orot_b200_geometry_source(void) { return kGeometrySource; }
 
 }  // extern "C"

@@ -8,6 +8,7 @@
 #include <vector>
 #include "engine.cuh"
 #include "kernels.cuh"
+#include "geometry_table.h"
 
 namespace orotb {
 
@@ -71,6 +72,7 @@ class Engine {
   // readable padding after the last byte).
   uint32_t checksum_device(uint32_t init, const uint8_t* d_data, size_t n, bool adler);
   uint32_t pick_tile(uint64_t total_bytes, int hash_bits) const;
+  const GeometryRow& geometry(uint64_t total_bytes) const;
 
   int device = 0, sms = 148;
   bool ok = false;  // the stream and the device's constant tables are set up

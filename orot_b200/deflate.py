@@ -67,6 +67,7 @@ def lib() -> ctypes.CDLL:
     L.deflate_adler32.restype = c.c_uint32
     L.deflate_adler32.argtypes = [c.c_uint32, c.c_void_p, c.c_size_t]
     L.orot_b200_last_error.restype = c.c_char_p
+    L.orot_b200_geometry_source.restype = c.c_char_p
     L.deflate_gpu_batch_new.restype = c.c_void_p
     L.deflate_gpu_batch_free.argtypes = [c.c_void_p]
     L.deflate_gpu_batch_load.restype = c.c_int
@@ -137,6 +138,11 @@ def lib() -> ctypes.CDLL:
 
 def last_error() -> str:
     return lib().orot_b200_last_error().decode()
+
+
+def geometry_source() -> str:
+    """Where the library's pass geometry table came from (the autotuner's run)."""
+    return lib().orot_b200_geometry_source().decode()
 
 
 def _ptr(buf) -> tuple[int, int, object]:
