@@ -91,7 +91,7 @@ def time_pass(deflate, torch, stream, data, sizes, level, env: dict, reps: int) 
 
 
 def write_table(rows, source: str, path: str = TABLE) -> None:
-    text = open(path).read()
+    text = open(TABLE).read()  # the header comment and struct stay as they are
     head = text[:text.index("constexpr const char* kGeometrySource")]
     body = [f'constexpr const char* kGeometrySource = "{source}";', "constexpr GeometryRow kGeometry[] = {"]
     for r in rows:
