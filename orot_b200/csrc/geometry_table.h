@@ -22,16 +22,16 @@ struct GeometryRow {
   uint32_t lazy_run[3];
 };
 
-constexpr const char* kGeometrySource = "hand-set rules (not yet tuned)";
+constexpr const char* kGeometrySource = "orot_b200.tune on NVIDIA B200, 148 SMs, 2026-12-04";
 constexpr GeometryRow kGeometry[] = {
-    {0ull, 8192, 16384, {1, 1, 1}},
-    {1ull << 20, 8192, 16384, {1, 1, 1}},
-    {4ull << 20, 8192, 16384, {2, 2, 2}},
-    {16ull << 20, 8192, 16384, {8, 8, 8}},
-    {64ull << 20, 8192, 16384, {16, 16, 16}},
-    {256ull << 20, 32768, 32768, {16, 16, 16}},
-    {1ull << 30, 65536, 65536, {32, 32, 32}},
-    {4ull << 30, 65536, 65536, {32, 32, 32}},
+    {0ull, 4096, 8192, {1, 1, 1}},
+    {1ull << 20, 4096, 8192, {2, 2, 2}},
+    {4ull << 20, 8192, 8192, {8, 8, 1}},
+    {16ull << 20, 16384, 32768, {4, 4, 2}},
+    {64ull << 20, 32768, 32768, {8, 8, 4}},
+    {256ull << 20, 32768, 65536, {16, 16, 16}},
+    {1ull << 30, 65536, 65536, {32, 32, 16}},
+    {4ull << 30, 65536, 65536, {32, 32, 16}},
 };
 
 }  // namespace orotb
