@@ -296,27 +296,38 @@ class OutRing:
 
 def _serve(deflate, srv, buf, trace, gaps, ring, expect=None):
     """Submits the trace (arrival gaps in seconds, or None for all at once)
-    and collects every result; returns latencies (s), the makespan from first
-    submission to last completion, and the results' CRC-32s.  With `expect`
-    (the CRC-32 and size of each request's single deflate_compress output),
-    every result is compared as it is collected."""
+    while a collector thread waits for the results in submission order,
+    frees their output space and, with `expect` (the CRC-32 and size of each
+    request's single deflate_compress output), compares every result.
+    Returns the latencies (s, submission to completion, timed by the server)
+    and the makespan from the first submission to the last completion."""
+    import queue
+    L = deflate.lib()
     sizes, levels, starts = trace
     n = len(sizes)
     lat = np.zeros(n)
-    crcs = [0] * n
-    pending = []  # (index, ticket, lo, hi) in submission order
+    sub_at = np.zeros(n)
+    q = queue.Queue()
+    cond = threading.Condition()
+    errors = []
+    base, rbase = buf.ctypes.data, ring.buf.ctypes.data
 
-    def collect_oldest():
-        i, t, lo, hi = pending.pop(0)
-        ring.regions.pop(0)
-        o, l = srv.wait(t, timeout=600)
-        if o is None:
-            raise SystemExit(f"served request {i} failed")
-        lat[i] = l
-        crcs[i] = (zlib.crc32(o), len(o))
-        if expect is not None and crcs[i] != expect[i]:
-            raise SystemExit(f"served request {i} differs from its single deflate_compress call")
+    def collector():
+        for _ in range(n):
+            i, t, lo = q.get()
+            sz, lt = ctypes.c_size_t(0), ctypes.c_double(0)
+            r = L.deflate_gpu_server_wait(srv._s, t, ctypes.byref(sz), ctypes.byref(lt), 600.0)
+            lat[i] = lt.value
+            if r != 0:
+                errors.append(f"served request {i} failed ({r})")
+            elif expect is not None and (zlib.crc32(ring.buf[lo:lo + sz.value]), int(sz.value)) != expect[i]:
+                errors.append(f"served request {i} differs from its single deflate_compress call")
+            with cond:
+                ring.regions.pop(0)
+                cond.notify_all()
 
+    th = threading.Thread(target=collector, daemon=True)
+    th.start()
     t0 = time.perf_counter()
     due = t0
     for i in range(n):
@@ -325,13 +336,18 @@ def _serve(deflate, srv, buf, trace, gaps, ring, expect=None):
             now = time.perf_counter()
             if due > now:
                 time.sleep(due - now)
-        cap = deflate.compress_bound(sizes[i], deflate.Format.Raw)
-        lo, hi = ring.take(cap, collect_oldest)
-        t = srv.submit(buf[starts[i]:starts[i] + sizes[i]], levels[i], deflate.Format.Raw, out=ring.buf[lo:hi])
-        pending.append((i, t, lo, hi))
-    while pending:
-        collect_oldest()
-    return lat, time.perf_counter() - t0, crcs
+        cap = deflate_bound(sizes[i])
+        with cond:
+            lo, hi = ring.take(cap, lambda: cond.wait(1.0))
+        sub_at[i] = time.perf_counter()
+        t = L.deflate_gpu_server_submit(srv._s, base + starts[i], sizes[i], rbase + lo, cap, levels[i], 0)
+        if t == 0:
+            raise SystemExit(f"submit {i} failed: {deflate.last_error()}")
+        q.put((i, t, lo))
+    th.join()
+    if errors:
+        raise SystemExit(errors[0])
+    return lat, float(np.max(sub_at + lat)) - t0
 
 
 def _single_outputs(L, buf, trace, idx, threads=16):
@@ -411,7 +427,7 @@ def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
     res = {"requests": count, "rate_req_s": rate, "offered_GBps": nbytes / gaps.sum() / 1e9,
            "duration_s": float(gaps.sum()), "bytes": nbytes, "levels": "70% L1 / 30% L6", "format": "raw",
            "sizes": "log-uniform 4 KiB-16 MiB", "budget_GiB": 16}
-    lat, span, _ = _serve(deflate, srv, buf, trace, gaps, ring, expect)
+    lat, span = _serve(deflate, srv, buf, trace, gaps, ring, expect)
     lat_ms = lat * 1e3
     res["open_loop"] = {"sustained_GBps": nbytes / span / 1e9, "p50_ms": float(np.percentile(lat_ms, 50)),
                         "p99_ms": float(np.percentile(lat_ms, 99)), "p999_ms": float(np.percentile(lat_ms, 99.9)),
@@ -423,7 +439,7 @@ def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
     for name, lv in (("mix", mix[:k]), ("L1", [1] * k), ("L6", [6] * k)):
         tr = (sizes[:k], lv, starts[:k])
         exp = expect[:k] if name == "mix" else None
-        lat, span, _ = _serve(deflate, srv, buf, tr, None, ring, exp)
+        lat, span = _serve(deflate, srv, buf, tr, None, ring, exp)
         plain = _plain(L, buf, tr, sample)
         kb = sum(sizes[:k])
         cap[name] = {"requests": k, "GBps": kb / span / 1e9, "p50_ms": float(np.percentile(lat * 1e3, 50)),

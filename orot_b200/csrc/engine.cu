@@ -45,8 +45,25 @@ int clamp_level(int l) { return l < 0 ? 0 : l > 12 ? 12 : l; }
 
 bool DevBuf::ensure(size_t n) {
   if (n <= cap) return true;
-  size_t want = std::max(n, cap + cap / 2);  // grow geometrically: cudaFree synchronises the device
-  if (p) cudaFree(p);
+  size_t want = std::max(n, cap + cap / 2);  // grow geometrically
+  if (pool) {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    cap = 0;
+    if (cudaMallocFromPoolAsync(&p, want, pool, st) != cudaSuccess) {
+      cudaGetLastError();
+      if (cudaMallocFromPoolAsync(&p, n, pool, st) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        set_error("device arena allocation failed");
+        return false;
+      }
+      want = n;
+    }
+    cap = want;
+    return true;
+  }
+  if (p) cudaFree(p);  // synchronises the device
   p = nullptr;
   cap = 0;
   if (cudaMalloc(&p, want) != cudaSuccess) {
@@ -57,7 +74,51 @@ bool DevBuf::ensure(size_t n) {
   cap = want;
   return true;
 }
-void DevBuf::release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+void DevBuf::release() {
+  if (p) {
+    if (pool) cudaFreeAsync(p, st);
+    else cudaFree(p);
+  }
+  p = nullptr;
+  cap = 0;
+}
+
+// The arena memory pool of a device (the calling thread's current one): a
+// pool of this library's own that keeps freed memory for reuse instead of
+// returning it at every synchronisation; nullptr when the device has none.
+static cudaMemPool_t arena_pool(int dev) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  static bool tried[64] = {};
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!tried[dev]) {
+    tried[dev] = true;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pl = nullptr;
+    if (cudaMemPoolCreate(&pl, &props) == cudaSuccess) {
+      uint64_t keep = ~uint64_t(0);
+      cudaMemPoolSetAttribute(pl, cudaMemPoolAttrReleaseThreshold, &keep);
+      pools[dev] = pl;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  return pools[dev];
+}
+
+void Engine::use_stream_ordered_arenas() {
+  cudaMemPool_t pl = arena_pool(device);
+  if (!pl) return;
+  for (DevBuf* b : {&d_in, &d_out, &d_scratch, &d_tables, &d_pack}) {
+    if (b->p) continue;  // only arenas not yet allocated change mode
+    b->pool = pl;
+    b->st = stream;
+  }
+}
 
 bool HostBuf::ensure(size_t n) {
   if (n <= cap) return true;
@@ -97,6 +158,7 @@ Engine::Engine() {
 Engine::~Engine() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   for (DevBuf* b : {&d_in, &d_out, &d_scratch, &d_tables, &d_pack}) b->release();
+  if (stream) cudaStreamSynchronize(stream);
   h_tables.release();
   h_stage.release();
   if (stream) cudaStreamDestroy(stream);
@@ -134,7 +196,11 @@ bool Engine::plan(const std::vector<Job>& jobs) {
   streams.clear(); segs.clear(); tiles.clear(); cks.clear();
   for (auto& l : lists) l.clear();
   uint64_t total = 0;
-  for (const Job& j : jobs) total += j.in_len;
+  max_out_cap = 0;
+  for (const Job& j : jobs) {
+    total += j.in_len;
+    max_out_cap = std::max<uint64_t>(max_out_cap, j.out_cap);
+  }
   const uint32_t T12 = pick_tile(total, 12), T14 = pick_tile(total, 14);
   uint64_t scratch = 0;
   uint32_t npieces = 0;
@@ -226,6 +292,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
         scratch += 1024;
       }
       const uint32_t stored_pieces = std::max<uint32_t>(1, uint32_t((len + 65534) / 65535));
+      g.piece_off = npieces - s.piece_first;
       npieces += 1 + 2 * g.tile_count + 2 + 3 * stored_pieces;
       segs.push_back(g);
     }
@@ -361,7 +428,7 @@ bool Engine::launch(cudaStream_t st) {
     L.counter = counters + 2;
     launches += launch_lazy(w, L, st, sms, &marks);
   }
-  launch_plan(w, st);
+  launch_plan(w, max_out_cap, st);
   marks.mark(kPhPlan, st);
   launches += 2;
   launch_join(w, counters + 3, st, sms);
@@ -407,39 +474,50 @@ size_t parallel_bound(size_t n, int fmt, int level, size_t block) {
   return std::max(framed_bound(n, fmt), n + nchunk * (5 * pieces + 1) + 32);
 }
 
+// Pinned staging of a one-call entry point is sized at least this much, so
+// that the first calls do not each grow it (pinning memory is slow).
+constexpr size_t kStageMin = size_t(4) << 20;
+// Below this output bound, the result record and the whole output slot come
+// back in one device-to-host round trip (one wait instead of two).
+constexpr size_t kOneTripBound = size_t(1) << 20;
+
 size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, int level, int fmt, bool parallel,
                              size_t block, uint32_t mode, Stream* result) {
   const size_t bound = parallel ? parallel_bound(n, fmt, level, block) : framed_bound(n, fmt);
   if (!ensure_io(align_up(n, 16), align_up(bound, 16))) return 0;
+  if (!h_stage.ensure(std::max({n, bound + 64, kStageMin}))) return 0;
+  uint8_t* stage = static_cast<uint8_t*>(h_stage.p);
   if (n) {
-    if (!h_stage.ensure(n)) return 0;
-    std::memcpy(h_stage.p, in, n);
-    if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) { set_error("H2D failed"); return 0; }
+    std::memcpy(stage, in, n);
+    if (cudaMemcpyAsync(d_in.p, stage, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) { set_error("H2D failed"); return 0; }
   }
   std::vector<Job> jobs(1);
   jobs[0] = Job{0, n, 0, parallel ? std::min<uint64_t>(cap, bound) : bound, level, fmt, parallel, block, mode};
   if (!plan(jobs) || !launch(stream)) return 0;
+  const bool one_trip = bound <= kOneTripBound;
   Stream s{};
   if (cudaMemcpyAsync(&s, static_cast<uint8_t*>(d_tables.p) + off_streams, sizeof s, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      (one_trip && cudaMemcpyAsync(stage, d_out.p, bound, cudaMemcpyDeviceToHost, stream) != cudaSuccess) ||
       cudaStreamSynchronize(stream) != cudaSuccess) {
     set_error(std::string("device error: ") + cudaGetErrorString(cudaGetLastError()));
     return 0;
   }
   if (result) *result = s;
   if (s.error || s.out_size == 0 || s.out_size > cap) return 0;
-  if (!h_stage.ensure(s.out_size)) return 0;
-  if (cudaMemcpyAsync(h_stage.p, static_cast<uint8_t*>(d_out.p) + s.out_off, s.out_size, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-      cudaStreamSynchronize(stream) != cudaSuccess) {
-    set_error("D2H failed");
-    return 0;
+  if (!one_trip) {
+    if (cudaMemcpyAsync(stage, static_cast<uint8_t*>(d_out.p) + s.out_off, s.out_size, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+      set_error("D2H failed");
+      return 0;
+    }
   }
-  std::memcpy(out, h_stage.p, s.out_size);
+  std::memcpy(out, stage + (one_trip ? s.out_off : 0), s.out_size);
   return s.out_size;
 }
 
 uint32_t Engine::checksum_host(uint32_t init, const void* data, size_t n, bool adler) {
   if (n == 0) return init;
-  if (!ensure_io(align_up(n, 16), 64) || !h_stage.ensure(n)) return init;
+  if (!ensure_io(align_up(n, 16), 64) || !h_stage.ensure(std::max(n, kStageMin))) return init;
   std::memcpy(h_stage.p, data, n);
   if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
     set_error("H2D failed");
@@ -525,6 +603,7 @@ EngineLease::EngineLease() {
   lk.unlock();
   Engine* e = new (std::nothrow) Engine();  // binds to this thread's current device, dev_
   if (e && e->ok) {
+    e->use_stream_ordered_arenas();  // its work runs on its own stream only
     e_ = e;
     return;
   }

@@ -67,7 +67,7 @@ struct Segment {
   uint32_t eob;        // EOB code | (code length << 16)
   // filled by the planner kernel
   uint32_t block_type;
-  uint32_t pad0;
+  uint32_t piece_off;  // first copy slot of this block, from the stream's piece_first
   uint64_t bit_off;    // block start, in bits from the stream's raw start
   uint64_t bits;       // block length in bits (stored: for its actual offset)
 };

@@ -19,9 +19,16 @@ size_t default_block(int level);
 size_t parallel_bound(size_t n, int fmt, int level, size_t block);
 int clamp_level(int l);
 
+// A device arena that grows on demand.  With `pool` set, it grows by
+// stream-ordered allocation on `st` (the only stream that uses it), which
+// does not synchronise the device; otherwise by cudaMalloc / cudaFree, which
+// waits for all work on the device (used where another stream may still be
+// reading the old arena, e.g. a batch run on a caller's stream).
 struct DevBuf {
   void* p = nullptr;
   size_t cap = 0;
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t st = nullptr;
   bool ensure(size_t n);
   void release();
 };
@@ -71,6 +78,9 @@ class Engine {
   // Checksum of n bytes already on the device (d_data 16-byte aligned, with
   // readable padding after the last byte).
   uint32_t checksum_device(uint32_t init, const uint8_t* d_data, size_t n, bool adler);
+  // Makes the arenas grow by stream-ordered allocation on the engine's own
+  // stream (for engines whose work runs on that stream only).
+  void use_stream_ordered_arenas();
   uint32_t pick_tile(uint64_t total_bytes, int hash_bits) const;
   const GeometryRow& geometry(uint64_t total_bytes) const;
 
@@ -91,6 +101,7 @@ class Engine {
   std::vector<uint32_t> lists[kNumLists];
   uint32_t n_pieces = 0;
   uint64_t scratch_bytes = 0, upload_bytes = 0;
+  uint64_t max_out_cap = 0;  // largest output slot of the planned pass
   uint64_t off_streams = 0, off_segs = 0, off_tiles = 0, off_ck = 0, off_pieces = 0, off_counters = 0;
   uint64_t off_lists[kNumLists] = {};
   int launches = 0;

@@ -1,11 +1,21 @@
 // kernels.cuh -- launch interface between the host engine and the kernels.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include "engine.cuh"
 #include "deflate_device.cuh"
 
 namespace orotb {
+
+// Index of the calling thread's current device for per-device launch caches
+// (kernel attributes and occupancy are properties of a device and never
+// change, so they are set and queried on a device's first launch only).
+inline int device_slot() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) d = 0;
+  return d;
+}
 
 // Device pointers of one compression pass.
 struct Work {
@@ -60,7 +70,7 @@ struct Marks {
 
 void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms, Marks* mk);
 int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms, Marks* mk);
-void launch_plan(const Work& wk, cudaStream_t st);
+void launch_plan(const Work& wk, uint64_t max_out, cudaStream_t st);  // max_out: largest stream bound
 void launch_checksums(const Work& wk, cudaStream_t st);
 void launch_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total, uint32_t init, int adler, uint32_t* res,
                       const Work& wk, cudaStream_t st);

@@ -1,19 +1,22 @@
 // kernels_common.cu -- block planning, output assembly and checksums.
 //
-//   k_plan      one thread per stream: block type of every segment (the
-//               reference's rules, src/deflate/deflate_block.cpp:389-474 and
+//   k_plan_*    block type of every segment (the reference's rules,
+//               src/deflate/deflate_block.cpp:389-474 and
 //               src/compress/block_compressor.cpp:53-63), bit offset of every
 //               block, and the list of bit-range copies that assemble the
-//               stream; output size and capacity check.
-//   k_zero      clears the words the stream will occupy.
+//               stream; output size and capacity check (one warp per segment
+//               or stream, see below).
+//   k_zero      clears the words the streams will occupy.
 //   k_ck_block  CRC-32 (slicing-by-4) and Adler-32 partial sums of 64 KiB
 //               blocks, 256 bytes per thread, folded with the GF(2) shift /
 //               Adler weight identities.
-//   k_ck_fold   folds the blocks of each stream in order.
+//   k_ck_fold   folds the blocks of each stream: runs of blocks per thread,
+//               then a tree over the runs (one CTA per stream).
 //   k_join      one warp per copy: funnel-shifted 32-bit words, plain stores
 //               inside a copy, atomicOr on the two boundary words it shares.
 //   k_frame     zlib / gzip header and trailer bytes.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <mutex>
 #include <cstdint>
 #include "engine.cuh"
@@ -27,122 +30,198 @@ constexpr uint32_t kFullMask = 0xFFFFFFFFu;
 __host__ __device__ inline uint32_t fmt_header_bytes(uint32_t fmt) { return fmt == kFmtZlib ? 2 : fmt == kFmtGzip ? 10 : 0; }
 __host__ __device__ inline uint32_t fmt_trailer_bytes(uint32_t fmt) { return fmt == kFmtZlib ? 4 : fmt == kFmtGzip ? 8 : 0; }
 
-// ---------------------------------------------------------------- k_plan
-__device__ __forceinline__ void put_piece(Piece* pc, uint32_t& k, uint32_t kmax, const uint32_t* src, uint32_t* dst,
-                                          uint64_t sbit, uint64_t dbit, uint32_t nbits, uint32_t value) {
-  if (nbits == 0) return;
-  if (k < kmax) pc[k] = Piece{src, dst, sbit, dbit, nbits, value};
-  ++k;
+// ---------------------------------------------------------------- planning
+// Three kernels, so that a stream of thousands of segments (a pigz-style
+// stream) or a segment of thousands of tiles (a large whole buffer) is
+// planned in parallel:
+//   k_plan_seg     one warp per segment: token bits and matches summed over
+//                  its tiles, the block type, and the block's length when it
+//                  does not depend on its bit alignment (Huffman blocks).
+//   k_plan_stream  one warp per stream: block offsets in order (32 segments
+//                  loaded at a time, followed through shuffles; a stored
+//                  block's padding depends on where it starts), stream size,
+//                  capacity check, the closing sync point of an open part.
+//   k_plan_pieces  one warp per segment: its bit-range copies, at slots the
+//                  host reserved for the segment (Segment::piece_off); unused
+//                  slots are left empty (nbits 0).
+
+// Bits a stored block of `len` bytes starting at bit c occupies: per piece of
+// at most 65535 bytes, 3 header bits, padding to a byte, LEN/NLEN and the
+// bytes (deflate_block.cpp:107-132).
+__device__ __forceinline__ uint64_t stored_bits_at(uint64_t c, uint32_t len) {
+  const uint64_t pieces = len ? (uint64_t(len) + 65534) / 65535 : 1;
+  return (((c + 3 + 7) & ~uint64_t(7)) - c) + 32 + uint64_t(len) * 8 + (pieces - 1) * 40;
 }
 
-__global__ void k_plan(Work wk) {
-  const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ uint32_t seg_piece_slots(const Segment& sg) {
+  const uint32_t stored_pieces = max(1u, (sg.len + 65534u) / 65535u);
+  return 1 + 2 * sg.tile_count + 2 + 3 * stored_pieces;
+}
+
+__global__ void k_plan_seg(Work wk) {
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (g >= wk.nsegs) return;
+  const Segment sg = wk.segs[g];
+  unsigned long long tok = 0, matches = 0;
+  if (sg.level > 0) {
+    for (uint32_t t = sg.tile_first + lane; t < sg.tile_first + sg.tile_count; t += 32) {
+      const Tile& tl = wk.tiles[t];
+      tok += uint64_t(tl.fix_bits) + (tl.spec_bits - tl.splice_bit);
+      matches += tl.fin_matches;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    tok += __shfl_xor_sync(kFullMask, tok, o);
+    matches += __shfl_xor_sync(kFullMask, matches, o);
+  }
+  if (lane) return;
+  uint32_t type = kBlkStored;
+  uint64_t bits = 0;
+  if (sg.level > 0) {
+    if (sg.level >= 4) {
+      type = sg.block_type;  // chosen by the lazy pipeline
+    } else if ((sg.flags & kSegWholeBuf) && matches == 0) {
+      type = kBlkStored;     // all-literal parse (block_compressor.cpp:60-61)
+    } else {
+      const uint64_t fixed_bits = 3 + tok + 7;      // header + tokens + EOB
+      const uint64_t stored = (uint64_t(sg.len) + 5) * 8;
+      type = stored <= fixed_bits ? kBlkStored : kBlkFixed;
+    }
+  }
+  if (type == kBlkFixed) bits = 3 + tok + 7;                       // EOB is code 0000000
+  else if (type == kBlkDynamic) bits = 3 + sg.hdr_bits + tok + (sg.eob >> 16);
+  wk.segs[g].block_type = type;
+  wk.segs[g].bits = bits;
+}
+
+__global__ void k_plan_stream(Work wk) {
+  const uint32_t si = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (si >= wk.nstreams) return;
   Stream s = wk.streams[si];
   const bool bare = (s.mode & kStreamBare) != 0;
   const uint32_t hdr = bare ? 0 : fmt_header_bytes(s.fmt), trl = bare ? 0 : fmt_trailer_bytes(s.fmt);
-  uint32_t* dst = reinterpret_cast<uint32_t*>(wk.out + s.out_off);
-  Piece* pc = wk.pieces + s.piece_first;
-  uint32_t k = 0;
-  const uint32_t kmax = s.piece_count;
-  const uint64_t base = uint64_t(hdr) * 8;
   uint64_t c = 0;  // bits from the start of the raw DEFLATE stream
-  bool bad = false;
-  for (uint32_t g = s.seg_first; g < s.seg_first + s.seg_count; ++g) {
-    Segment sg = wk.segs[g];
-    const bool last = (sg.flags & kSegLast) != 0;
-    uint32_t type = kBlkStored;
-    uint64_t tok_bits = 0, matches = 0;
-    if (sg.level > 0) {
-      for (uint32_t t = sg.tile_first; t < sg.tile_first + sg.tile_count; ++t) {
-        const Tile& tl = wk.tiles[t];
-        tok_bits += uint64_t(tl.fix_bits) + (tl.spec_bits - tl.splice_bit);
-        matches += tl.fin_matches;
-      }
-      if (sg.level >= 4) {
-        type = sg.block_type;  // chosen by the lazy pipeline
-      } else if ((sg.flags & kSegWholeBuf) && matches == 0) {
-        type = kBlkStored;     // all-literal parse (block_compressor.cpp:60-61)
-      } else {
-        const uint64_t fixed_bits = 3 + tok_bits + 7;      // header + tokens + EOB
-        const uint64_t stored_bits = (uint64_t(sg.len) + 5) * 8;
-        type = stored_bits <= fixed_bits ? kBlkStored : kBlkFixed;
-      }
+  for (uint32_t g0 = s.seg_first; g0 < s.seg_first + s.seg_count; g0 += 32) {
+    const uint32_t cnt = min(32u, s.seg_first + s.seg_count - g0);
+    uint32_t type = 0, len = 0, last = 0;
+    uint64_t bits = 0;
+    if (lane < cnt) {
+      const Segment& sg = wk.segs[g0 + lane];
+      type = sg.block_type;
+      len = sg.len;
+      last = sg.flags & kSegLast;
+      bits = sg.bits;
     }
-    const uint64_t start = c;
-    if (type == kBlkStored) {
-      uint32_t off = 0;
-      for (;;) {
-        const uint32_t n = min(sg.len - off, 65535u);
-        const bool fin = last && off + n == sg.len;
-        put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 3, fin ? 1u : 0u);
-        c += 3;
-        c = (c + 7) & ~uint64_t(7);
-        put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 32, n | ((~n & 0xFFFFu) << 16));
-        c += 32;
-        const uint64_t a = sg.in_off + off;
-        put_piece(pc, k, kmax, reinterpret_cast<const uint32_t*>(wk.in + (a & ~uint64_t(3))), dst, (a & 3) * 8,
-                  base + c, n * 8, 0);
-        c += uint64_t(n) * 8;
-        off += n;
-        if (n == 0 || off >= sg.len) break;
-      }
-    } else {
-      // BFINAL + BTYPE (write_bits(type, 2) puts the low bit first)
-      if (type == kBlkFixed) {
-        put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 3, (last ? 1u : 0u) | (1u << 1));
-        c += 3;
-      } else {
-        // code-length header written by the Huffman kernel
-        const uint32_t* hsrc = reinterpret_cast<const uint32_t*>(wk.scratch + sg.hdr_off);
-        put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 3, (last ? 1u : 0u) | (2u << 1));
-        c += 3;
-        put_piece(pc, k, kmax, hsrc, dst, 0, base + c, sg.hdr_bits, 0);
-        c += sg.hdr_bits;
-      }
-      for (uint32_t t = sg.tile_first; t < sg.tile_first + sg.tile_count; ++t) {
-        const Tile& tl = wk.tiles[t];
-        const uint32_t* spec = reinterpret_cast<const uint32_t*>(wk.scratch + tl.scratch);
-        const uint32_t* fix = reinterpret_cast<const uint32_t*>(wk.scratch + tl.scratch + tile_stream_bytes(tl.len));
-        put_piece(pc, k, kmax, fix, dst, 0, base + c, tl.fix_bits, 0);
-        c += tl.fix_bits;
-        put_piece(pc, k, kmax, spec, dst, tl.splice_bit, base + c, tl.spec_bits - tl.splice_bit, 0);
-        c += tl.spec_bits - tl.splice_bit;
-      }
-      if (type == kBlkFixed) {
-        c += 7;  // EOB is code 0000000
-      } else {
-        const uint32_t eob = sg.eob;  // dynamic EOB: code | (len << 16)
-        put_piece(pc, k, kmax, nullptr, dst, 0, base + c, eob >> 16, eob & 0xFFFFu);
-        c += eob >> 16;
-      }
+    uint64_t my_off = 0, my_bits = 0;
+    for (uint32_t j = 0; j < cnt; ++j) {
+      const uint32_t tj = __shfl_sync(kFullMask, type, j), lj = __shfl_sync(kFullMask, len, j);
+      const uint32_t fj = __shfl_sync(kFullMask, last, j);
+      const uint64_t bj = __shfl_sync(kFullMask, bits, j);
+      const uint64_t start = c;
+      c += tj == kBlkStored ? stored_bits_at(c, lj) : bj;
+      if (fj) c = (c + 7) & ~uint64_t(7);
+      if (lane == j) { my_off = start; my_bits = c - start; }
     }
-    if (last) c = (c + 7) & ~uint64_t(7);
-    sg.block_type = type;
-    sg.bit_off = start;
-    sg.bits = c - start;
-    wk.segs[g] = sg;
+    if (lane < cnt) {
+      wk.segs[g0 + lane].bit_off = my_off;
+      wk.segs[g0 + lane].bits = my_bits;
+    }
   }
-  if (s.mode & kStreamOpen) {
-    // sync point: empty stored block, BFINAL = 0, LEN 0000 NLEN FFFF
-    put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 3, 0u);
-    c = (c + 3 + 7) & ~uint64_t(7);
-    put_piece(pc, k, kmax, nullptr, dst, 0, base + c, 32, 0xFFFF0000u);
-    c += 32;
-  }
-  bad = k > kmax;
+  if (lane) return;
+  Piece* tail = wk.pieces + s.piece_first + s.piece_count - 2;  // the open part's sync point
+  const uint64_t sync_at = c;
+  if (s.mode & kStreamOpen) c = ((c + 3 + 7) & ~uint64_t(7)) + 32;  // empty stored block, BFINAL = 0
   const uint64_t size = uint64_t(hdr) + c / 8 + trl;
   s.raw_bits = c;
-  s.error = kErrNone;
-  if (bad) s.error = kErrInternal;
-  else if (size > s.out_cap) s.error = kErrCapacity;
+  s.error = size > s.out_cap ? kErrCapacity : kErrNone;
   s.out_size = s.error ? 0 : size;
-  if (s.error) k = 0;
-  for (uint32_t i = (k < kmax ? k : kmax); i < kmax; ++i) pc[i].nbits = 0;
+  if (s.mode & kStreamOpen) {
+    uint32_t* dst = reinterpret_cast<uint32_t*>(wk.out + s.out_off);
+    const uint64_t base = uint64_t(hdr) * 8;
+    tail[0] = Piece{nullptr, dst, 0, base + sync_at, s.error ? 0u : 3u, 0u};
+    tail[1] = Piece{nullptr, dst, 0, base + ((sync_at + 3 + 7) & ~uint64_t(7)), s.error ? 0u : 32u, 0xFFFF0000u};
+  }
   wk.streams[si] = s;
 }
 
+__global__ void k_plan_pieces(Work wk) {
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (g >= wk.nsegs) return;
+  const Segment sg = wk.segs[g];
+  const Stream& s = wk.streams[sg.stream];
+  const bool bare = (s.mode & kStreamBare) != 0;
+  const uint32_t hdr = bare ? 0 : fmt_header_bytes(s.fmt);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(wk.out + s.out_off);
+  Piece* pc = wk.pieces + s.piece_first + sg.piece_off;
+  const uint32_t slots = seg_piece_slots(sg);
+  const uint64_t c = uint64_t(hdr) * 8 + sg.bit_off;  // block start in the output slot
+  const bool last = (sg.flags & kSegLast) != 0;
+  for (uint32_t i = lane; i < slots; i += 32) pc[i].nbits = 0;
+  __syncwarp();
+  if (s.error) return;
+  if (sg.block_type == kBlkStored) {
+    const uint32_t P = max(1u, (sg.len + 65534u) / 65535u);
+    const uint64_t c1 = ((c + 3 + 7) & ~uint64_t(7)) + 32 + 8ull * 65535;  // start of piece 1 (when P > 1)
+    for (uint32_t i = lane; i < P; i += 32) {
+      const uint64_t ci = i == 0 ? c : c1 + uint64_t(i - 1) * (40 + 8ull * 65535);
+      const uint32_t off = i * 65535u, n = min(sg.len - off, 65535u);
+      const bool fin = last && off + n == sg.len;
+      const uint64_t lenpos = (ci + 3 + 7) & ~uint64_t(7);
+      const uint64_t a = sg.in_off + off;
+      pc[3 * i] = Piece{nullptr, dst, 0, ci, 3, fin ? 1u : 0u};
+      pc[3 * i + 1] = Piece{nullptr, dst, 0, lenpos, 32, n | ((~n & 0xFFFFu) << 16)};
+      pc[3 * i + 2] = Piece{reinterpret_cast<const uint32_t*>(wk.in + (a & ~uint64_t(3))), dst, (a & 3) * 8,
+                            lenpos + 32, n * 8, 0};
+    }
+    return;
+  }
+  // BFINAL + BTYPE (write_bits(type, 2) puts the low bit first), then the
+  // code-length header of a dynamic block (written by the Huffman kernel)
+  uint64_t at = c + 3;
+  if (lane == 0) pc[0] = Piece{nullptr, dst, 0, c, 3, (last ? 1u : 0u) | (sg.block_type << 1)};
+  if (sg.block_type == kBlkDynamic) {
+    if (lane == 0)
+      pc[1] = Piece{reinterpret_cast<const uint32_t*>(wk.scratch + sg.hdr_off), dst, 0, at, sg.hdr_bits, 0};
+    at += sg.hdr_bits;
+  }
+  // two copies per tile (fix-up bits, then the speculative bits from the
+  // splice point), at offsets from a prefix sum over the tiles
+  for (uint32_t t0 = 0; t0 < sg.tile_count; t0 += 32) {
+    const uint32_t t = t0 + lane;
+    uint32_t fb = 0, sb = 0, sp = 0;
+    const Tile* tl = nullptr;
+    if (t < sg.tile_count) {
+      tl = wk.tiles + sg.tile_first + t;
+      fb = tl->fix_bits;
+      sp = tl->splice_bit;
+      sb = tl->spec_bits - sp;
+    }
+    unsigned long long incl = uint64_t(fb) + sb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long v = __shfl_up_sync(kFullMask, incl, o);
+      if (lane >= uint32_t(o)) incl += v;
+    }
+    const uint64_t mine = at + incl - (uint64_t(fb) + sb);
+    if (tl) {
+      const uint32_t* spec = reinterpret_cast<const uint32_t*>(wk.scratch + tl->scratch);
+      const uint32_t* fix = reinterpret_cast<const uint32_t*>(wk.scratch + tl->scratch + tile_stream_bytes(tl->len));
+      pc[2 + 2 * t] = Piece{fix, dst, 0, mine, fb, 0};
+      pc[3 + 2 * t] = Piece{spec, dst, sp, mine + fb, sb, 0};
+    }
+    at += __shfl_sync(kFullMask, incl, 31);
+  }
+  if (lane == 0 && sg.block_type == kBlkDynamic) {
+    const uint32_t eob = sg.eob;  // dynamic EOB: code | (len << 16)
+    pc[2 + 2 * sg.tile_count] = Piece{nullptr, dst, 0, at, eob >> 16, eob & 0xFFFFu};
+  }
+}
+
 // ---------------------------------------------------------------- k_zero
+// Clears the words every stream will occupy (the join ORs boundary words):
+// blockIdx.y splits a stream into gridDim.y parts, so one large stream is
+// cleared by many CTAs.
 __global__ void k_zero(Work wk) {
   const uint32_t si = blockIdx.x;
   if (si >= wk.nstreams) return;
@@ -150,7 +229,9 @@ __global__ void k_zero(Work wk) {
   if (s.error) return;
   uint4* o = reinterpret_cast<uint4*>(wk.out + s.out_off);
   const uint64_t n16 = (s.out_size + 15) / 16;
-  for (uint64_t i = threadIdx.x; i < n16; i += blockDim.x) o[i] = make_uint4(0, 0, 0, 0);
+  const uint64_t per = (n16 + gridDim.y - 1) / gridDim.y;
+  const uint64_t b = per * blockIdx.y, e = min(n16, b + per);
+  for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) o[i] = make_uint4(0, 0, 0, 0);
 }
 
 // ---------------------------------------------------------------- checksums
@@ -242,45 +323,92 @@ __global__ void __launch_bounds__(256) k_ck_block(Work wk, CrcPowers pw) {
   }
 }
 
-__global__ void k_ck_fold(Work wk, CrcPowers pw) {
-  const uint32_t si = blockIdx.x * blockDim.x + threadIdx.x;
-  if (si >= wk.nstreams) return;
-  Stream s = wk.streams[si];
-  if (s.fmt == kFmtRaw) return;
-  uint32_t crc = 0;
-  uint64_t s1 = 1, s2 = 0;
-  for (uint32_t i = s.ck_first; i < s.ck_first + s.ck_count; ++i) {
-    const CkBlock b = wk.ck[i];
-    const uint32_t shift = b.len == kCkBlock ? c_crc_block : xpow8n(pw, b.len);
-    crc = gf2_mulmod(shift, crc) ^ b.crc;
-    s2 = (s2 + uint64_t(b.len % kAdlerMod) * s1 + b.b) % kAdlerMod;
-    s1 = (s1 + b.a) % kAdlerMod;
+// Checksum partial of a byte range: the raw CRC register from 0, Adler sums
+// A = sum of bytes and B = sum of (len - i) * byte_i (mod 65521), and length.
+struct CkPartial {
+  uint32_t crc, a, b;
+  uint64_t len;
+};
+constexpr int kFoldThreads = 128;
+
+// Folds blocks blk[0, n) in order into one partial: every thread of the CTA
+// (kFoldThreads threads) folds a contiguous run of blocks, then the runs are
+// combined in a tree (appending R multiplies the CRC register by x^(8|R|) and
+// adds |R| * A to B).  Every thread must call it; thread 0 gets the result.
+__device__ CkPartial fold_blocks(const CkBlock* blk, uint32_t n, uint32_t what, const CrcPowers& pw,
+                                 CkPartial* sh) {
+  const uint32_t t = threadIdx.x;
+  const uint32_t per = (n + kFoldThreads - 1) / kFoldThreads;
+  const uint32_t b0 = min(n, t * per), b1 = min(n, b0 + per);
+  CkPartial p{0, 0, 0, 0};
+  for (uint32_t i = b0; i < b1; ++i) {
+    const CkBlock b = blk[i];
+    if (what & kCkCrc) p.crc = gf2_mulmod(b.len == kCkBlock ? c_crc_block : xpow8n(pw, b.len), p.crc) ^ b.crc;
+    if (what & kCkAdler) {
+      p.b = uint32_t((uint64_t(p.b) + uint64_t(b.len % kAdlerMod) * p.a + b.b) % kAdlerMod);
+      p.a = (p.a + b.a) % kAdlerMod;
+    }
+    p.len += b.len;
   }
+  sh[t] = p;
+  __syncthreads();
+  for (uint32_t s = 1; s < uint32_t(kFoldThreads); s <<= 1) {
+    if ((t & (2 * s - 1)) == 0 && t + s < uint32_t(kFoldThreads)) {
+      CkPartial l = sh[t];
+      const CkPartial r = sh[t + s];
+      if (r.len) {
+        if (what & kCkCrc) l.crc = gf2_mulmod(xpow8n(pw, r.len), l.crc) ^ r.crc;
+        if (what & kCkAdler) {
+          l.b = uint32_t((uint64_t(l.b) + (r.len % kAdlerMod) * l.a + r.b) % kAdlerMod);
+          l.a = (l.a + r.a) % kAdlerMod;
+        }
+        l.len += r.len;
+        sh[t] = l;
+      }
+    }
+    __syncthreads();
+  }
+  return sh[0];
+}
+
+// One CTA per stream.
+__global__ void __launch_bounds__(kFoldThreads) k_ck_fold(Work wk, CrcPowers pw) {
+  __shared__ CkPartial sh[kFoldThreads];
+  const uint32_t si = blockIdx.x;
+  if (si >= wk.nstreams) return;
+  const Stream& s = wk.streams[si];
+  if (s.fmt == kFmtRaw) return;
+  const uint32_t what = s.fmt == kFmtGzip ? kCkCrc : kCkAdler;
+  const CkPartial p = fold_blocks(wk.ck + s.ck_first, s.ck_count, what, pw, sh);
+  if (threadIdx.x) return;
+  uint32_t check;
   if (s.fmt == kFmtGzip) {
     // crc32(0, data) = ~(x^(8n) * ~0 + raw(data))
-    s.checksum = ~(gf2_mulmod(xpow8n(pw, s.in_len), 0xFFFFFFFFu) ^ crc);
+    check = ~(gf2_mulmod(xpow8n(pw, s.in_len), 0xFFFFFFFFu) ^ p.crc);
   } else {
-    s.checksum = uint32_t(s2 << 16) | uint32_t(s1);
+    // Adler-32 from 1: s1 = 1 + A, s2 = n + B
+    const uint64_t s1 = (1 + p.a) % kAdlerMod, s2 = (s.in_len % kAdlerMod + p.b) % kAdlerMod;
+    check = uint32_t(s2 << 16) | uint32_t(s1);
   }
-  wk.streams[si].checksum = s.checksum;
+  wk.streams[si].checksum = check;
 }
 
 // Single-stream checksum with an arbitrary initial value (deflate_crc32 /
-// deflate_adler32): result written to *res.
-__global__ void k_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total, uint32_t init, int adler, CrcPowers pw,
-                            uint32_t* res) {
-  if (threadIdx.x || blockIdx.x) return;
-  uint32_t crc = 0;
-  uint64_t s1 = (init & 0xFFFFu) % kAdlerMod, s2 = (init >> 16) % kAdlerMod;
-  for (uint32_t i = 0; i < nck; ++i) {
-    const CkBlock b = ck[i];
-    const uint32_t shift = b.len == kCkBlock ? c_crc_block : xpow8n(pw, b.len);
-    crc = gf2_mulmod(shift, crc) ^ b.crc;
-    s2 = (s2 + uint64_t(b.len % kAdlerMod) * s1 + b.b) % kAdlerMod;
-    s1 = (s1 + b.a) % kAdlerMod;
+// deflate_adler32): result written to *res.  One CTA.
+__global__ void __launch_bounds__(kFoldThreads) k_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total,
+                                                            uint32_t init, int adler, CrcPowers pw, uint32_t* res) {
+  __shared__ CkPartial sh[kFoldThreads];
+  if (blockIdx.x) return;
+  const CkPartial p = fold_blocks(ck, nck, adler ? kCkAdler : kCkCrc, pw, sh);
+  if (threadIdx.x) return;
+  if (adler) {
+    const uint64_t a0 = (init & 0xFFFFu) % kAdlerMod, b0 = (init >> 16) % kAdlerMod;
+    const uint64_t s1 = (a0 + p.a) % kAdlerMod;
+    const uint64_t s2 = (b0 + (total % kAdlerMod) * a0 + p.b) % kAdlerMod;
+    *res = uint32_t(s2 << 16) | uint32_t(s1);
+  } else {
+    *res = ~(gf2_mulmod(xpow8n(pw, total), ~init) ^ p.crc);
   }
-  if (adler) *res = uint32_t(s2 << 16) | uint32_t(s1);
-  else *res = ~(gf2_mulmod(xpow8n(pw, total), ~init) ^ crc);
 }
 
 // ---------------------------------------------------------------- k_join
@@ -393,23 +521,27 @@ CrcPowers host_crc_powers() {
   return pw;
 }
 
-void launch_plan(const Work& wk, cudaStream_t st) {
+void launch_plan(const Work& wk, uint64_t max_out, cudaStream_t st) {
   if (!wk.nstreams) return;
-  k_plan<<<(wk.nstreams + 127) / 128, 128, 0, st>>>(wk);
-  k_zero<<<wk.nstreams, 256, 0, st>>>(wk);
+  if (wk.nsegs) k_plan_seg<<<(wk.nsegs + 7) / 8, 256, 0, st>>>(wk);
+  k_plan_stream<<<(wk.nstreams + 7) / 8, 256, 0, st>>>(wk);
+  if (wk.nsegs) k_plan_pieces<<<(wk.nsegs + 7) / 8, 256, 0, st>>>(wk);
+  // about 1 MiB of output per clearing CTA for the largest stream
+  const uint32_t parts = uint32_t(std::min<uint64_t>(256, std::max<uint64_t>(1, max_out >> 20)));
+  k_zero<<<dim3(wk.nstreams, parts), 256, 0, st>>>(wk);
 }
 
 void launch_checksums(const Work& wk, cudaStream_t st) {
   const CrcPowers pw = host_crc_powers();
   if (wk.nck) k_ck_block<<<wk.nck, 256, 0, st>>>(wk, pw);
-  if (wk.nstreams) k_ck_fold<<<(wk.nstreams + 127) / 128, 128, 0, st>>>(wk, pw);
+  if (wk.nstreams) k_ck_fold<<<wk.nstreams, kFoldThreads, 0, st>>>(wk, pw);
 }
 
 void launch_ck_single(const CkBlock* ck, uint32_t nck, uint64_t total, uint32_t init, int adler, uint32_t* res,
                       const Work& wk, cudaStream_t st) {
   const CrcPowers pw = host_crc_powers();
   if (nck) k_ck_block<<<nck, 256, 0, st>>>(wk, pw);
-  k_ck_single<<<1, 32, 0, st>>>(ck, nck, total, init, adler, pw, res);
+  k_ck_single<<<1, kFoldThreads, 0, st>>>(ck, nck, total, init, adler, pw, res);
 }
 
 void launch_join(const Work& wk, uint32_t* counter, cudaStream_t st, int sms) {

@@ -92,10 +92,23 @@ __global__ void __launch_bounds__(256) k_carry_scan(Work wk, const uint32_t* __r
   for (uint32_t si = blockIdx.y; si < nseg; si += gridDim.y) {
     const Segment sg = wk.segs[seglist[si]];
     uint32_t run = 0;
-    for (uint32_t k = 0; k + 1 < sg.tile_count; ++k) {
-      uint32_t* slot = reinterpret_cast<uint32_t*>(wk.scratch + wk.tiles[sg.tile_first + k].slot);
-      run = max(run, slot[h]);
-      slot[h] = run;
+    // eight tiles at a time: their loads are issued before the dependent
+    // running maximum and the stores (one memory latency per eight tiles)
+    constexpr uint32_t B = 8;
+    const uint32_t nt = sg.tile_count ? sg.tile_count - 1 : 0;
+    for (uint32_t k0 = 0; k0 < nt; k0 += B) {
+      uint32_t* slot[B];
+      uint32_t v[B];
+#pragma unroll
+      for (uint32_t j = 0; j < B; ++j)
+        slot[j] = k0 + j < nt ? reinterpret_cast<uint32_t*>(wk.scratch + wk.tiles[sg.tile_first + k0 + j].slot) : nullptr;
+#pragma unroll
+      for (uint32_t j = 0; j < B; ++j) v[j] = slot[j] ? slot[j][h] : 0u;
+#pragma unroll
+      for (uint32_t j = 0; j < B; ++j) {
+        run = max(run, v[j]);
+        if (slot[j]) slot[j][h] = run;
+      }
     }
   }
 }
@@ -576,21 +589,25 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
   // (49.7 KB each) four fit either way.
   constexpr int WARPS = HB <= 12 ? 17 : 1;
   const size_t tbl_bytes = size_t(H) * 4;
-  if (L.n_lastocc) {
+  const size_t wsm = size_t(WARPS) * walker_words<HB>() * 4;
+  // walker CTAs per SM, and the kernels' shared-memory limits, once per device
+  static std::atomic<int> walk_per_sm[64];
+  const int ds = device_slot();
+  int per_sm = walk_per_sm[ds].load(std::memory_order_relaxed);
+  if (!per_sm) {
     cudaFuncSetAttribute(k_lastocc<HB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tbl_bytes));
-    k_lastocc<HB><<<L.n_lastocc, 256, tbl_bytes, st>>>(wk, L.lastocc, L.n_lastocc);
+    cudaFuncSetAttribute(k_walk<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<HB, WARPS>, WARPS * 32, wsm);
+    if (per_sm < 1) per_sm = 1;
+    walk_per_sm[ds].store(per_sm, std::memory_order_relaxed);
   }
+  if (L.n_lastocc) k_lastocc<HB><<<L.n_lastocc, 256, tbl_bytes, st>>>(wk, L.lastocc, L.n_lastocc);
   if (L.n_multi) {
     dim3 g((H + 255) / 256, L.n_multi < 65535u ? L.n_multi : 65535u);
     k_carry_scan<HB><<<g, 256, 0, st>>>(wk, L.multi, L.n_multi);
   }
   mk->mark(kPhPre, st);
-  const size_t wsm = size_t(WARPS) * walker_words<HB>() * 4;
   if (L.n_walk) {
-    cudaFuncSetAttribute(k_walk<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm));
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<HB, WARPS>, WARPS * 32, wsm);
-    if (per_sm < 1) per_sm = 1;
     uint32_t blocks = uint32_t(per_sm) * uint32_t(sms);
     const uint32_t need = (L.n_walk + WARPS - 1) / WARPS;
     if (blocks > need) blocks = need;

@@ -569,7 +569,12 @@ void launch_inflate(const uint8_t* in, uint8_t* out, InflateJob* jobs, const uin
   uint32_t blocks = uint32_t(sms) * 4;  // 4 CTAs of 4 warps per SM (shared memory)
   const uint32_t need = (njobs + kInfWarps - 1) / kInfWarps;
   if (blocks > need) blocks = need;
-  cudaFuncSetAttribute(k_inflate, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kInfSmem));
+  static std::atomic<bool> attr_set[64];
+  const int ds = device_slot();
+  if (!attr_set[ds].load(std::memory_order_relaxed)) {
+    if (cudaFuncSetAttribute(k_inflate, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kInfSmem)) == cudaSuccess)
+      attr_set[ds].store(true, std::memory_order_relaxed);
+  }
   k_inflate<<<blocks, kInfWarps * 32, kInfSmem, st>>>(in, out, jobs, order, njobs, counter);
 }
 

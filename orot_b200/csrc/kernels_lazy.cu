@@ -958,7 +958,12 @@ __global__ void __launch_bounds__(kEncWarps * 32) k_enc(Work wk, const uint32_t*
 
 int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms, Marks* mk) {
   if (!L.n_tiles) return 0;
-  cudaFuncSetAttribute(k_lz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLz));
+  static std::atomic<bool> attr_set[64];
+  const int ds = device_slot();
+  if (!attr_set[ds].load(std::memory_order_relaxed)) {
+    if (cudaFuncSetAttribute(k_lz, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemLz)) == cudaSuccess)
+      attr_set[ds].store(true, std::memory_order_relaxed);
+  }
   k_lz<<<L.n_runs, 1024, kSmemLz, st>>>(wk, L.runs, L.n_runs);
   mk->mark(kPhLazyLz, st);
   k_huff<<<(L.n_segs + kHuffWarps - 1) / kHuffWarps, kHuffWarps * 32, 0, st>>>(wk, L.segs, L.n_segs);

@@ -53,6 +53,7 @@ struct Lane {
   std::vector<void*> reqs;  // server: the requests of this pass
   size_t first = 0;         // pipelined batch: first buffer of this pass
   Lane() {
+    eng.use_stream_ordered_arenas();  // a lane's work runs on its engine's stream only
     cudaEventCreateWithFlags(&ev_meta, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_data, cudaEventDisableTiming);
   }
