@@ -367,7 +367,7 @@ int deflate_gpu_batch_phase_ms(deflate_gpu_batch* b, float* ms, int max) {
 }
 
 const char* deflate_gpu_phase_name(int i) {
-  static const char* names[kNumPhases] = {"hash_carry", "walk", "fixup", "lazy_match", "lazy_huffman",
+  static const char* names[kNumPhases] = {"hash_carry", "candidates", "parse", "fixup", "lazy_match", "lazy_huffman",
                                           "lazy_encode", "plan", "join", "checksum", "frame"};
   return i >= 0 && i < int(kNumPhases) ? names[i] : "";
 }

@@ -248,13 +248,13 @@ bool Engine::plan(const std::vector<Job>& jobs) {
           const uint64_t sb = tile_stream_bytes(tl.len);
           tl.scratch = scratch;
           scratch += 2 * sb;  // speculative + fix-up bit buffers
-          if (t > 0) {
-            tl.rec = scratch;
-            scratch += align_up(uint64_t((tl.len + 31) / 32) * sizeof(WinRec), 256);
-            tl.cand = scratch;
-            scratch += align_up(uint64_t(tl.len) * 2 + 64, 256);
-            tl.carry = tiles.back().slot;
-          }
+          // window records and candidate distances (every tile: the parse
+          // kernel reads them; the fix-up reads those of tiles after the first)
+          tl.rec = scratch;
+          scratch += align_up(uint64_t((tl.len + 31) / 32) * sizeof(WinRec), 256);
+          tl.cand = scratch;
+          scratch += align_up(uint64_t(tl.len) * 2 + 64, 256);
+          if (t > 0) tl.carry = tiles.back().slot;
           if (t + 1 < nt) {
             tl.slot = scratch;
             scratch += uint64_t(H) * 4;
@@ -410,11 +410,11 @@ bool Engine::launch(cudaStream_t st) {
     L.n_multi = uint32_t(lists[g ? kMulti14 : kMulti12].size());
     L.walk = list(g ? kWalk14 : kWalk12);
     L.n_walk = uint32_t(lists[g ? kWalk14 : kWalk12].size());
-    L.counter = counters + g;  // walk: 0/1; fix-up round 1: 4/5 (counter + 4)
+    L.counter = counters + g;  // candidates: 0/1; fix-up round 1: 4/5 (+ 4); parse: 6/7 (+ 6)
     if (L.n_walk) {
       launch_fast(w, L, hbs[g], st, sms, &marks);
-      // k_lastocc; k_carry_scan, k_fix1, k_fix2 for multi-tile segments; k_walk
-      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 3 : 0) + 1;
+      // k_lastocc; k_carry_scan, k_fix1, k_fix2 for multi-tile segments; k_cand, k_parse
+      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 3 : 0) + 2;
     }
   }
   if (!lists[kLazyTiles].empty()) {
@@ -430,7 +430,7 @@ bool Engine::launch(cudaStream_t st) {
   }
   launch_plan(w, max_out_cap, st);
   marks.mark(kPhPlan, st);
-  launches += 2;
+  launches += 4;  // k_plan_seg, k_plan_stream, k_plan_pieces, k_zero
   launch_join(w, counters + 3, st, sms);
   marks.mark(kPhJoin, st);
   launches += w.npieces ? 1 : 0;

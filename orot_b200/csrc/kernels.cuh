@@ -54,7 +54,7 @@ struct LazyLists {
 };
 
 // Optional per-phase CUDA events: mark(id) records an event after phase id.
-enum Phase { kPhPre = 0, kPhWalk, kPhFix, kPhLazyLz, kPhLazyHuff, kPhLazyEnc, kPhPlan, kPhJoin, kPhCheck, kPhFrame,
+enum Phase { kPhPre = 0, kPhCand, kPhWalk, kPhFix, kPhLazyLz, kPhLazyHuff, kPhLazyEnc, kPhPlan, kPhJoin, kPhCheck, kPhFrame,
              kNumPhases };
 struct Marks {
   cudaEvent_t ev[kNumPhases + 1];

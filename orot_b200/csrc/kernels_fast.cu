@@ -11,13 +11,18 @@
 //
 //   k_lastocc     per tile, last position of every hash (shared atomics)
 //   k_carry_scan  per segment, exclusive prefix-max of those tables
-//   k_walk        one warp per tile: 32 positions per step; hash, __match_any
-//                 for same-hash lanes, head[] in shared memory, capped match
-//                 lengths per lane, greedy parse resolved with ballots, fixed
-//                 Huffman bits packed with shared atomics and flushed as
-//                 coalesced 128-byte stores.  The parse starts at the tile's
-//                 first byte (speculation) and one record per 32 positions
-//                 remembers where it entered that window.
+//   k_cand        one warp per tile, head[] in shared memory (18 walkers of
+//                 12.4 KB per SM at 12 hash bits): 32 positions per step;
+//                 hash, __match_any for same-hash lanes, head lookup and
+//                 insert; the candidate distance of every position (2 bytes)
+//                 and the run period of every 32-position window.
+//   k_parse       one warp per tile, no table (16 warps of 0.6 KB per CTA,
+//                 many CTAs per SM): capped match lengths per lane, greedy
+//                 parse resolved with ballots, fixed Huffman bits packed with
+//                 shared atomics and flushed as coalesced 128-byte stores.
+//                 The parse starts at the tile's first byte (speculation) and
+//                 one record per 32 positions remembers where it entered that
+//                 window; windows a match covers cost only that record.
 //   k_fixup       one warp per multi-tile segment, tiles in order: re-walks a
 //                 tile from the true entry (where the previous tile's parse
 //                 ended) until it meets the speculative parse at a window
@@ -452,15 +457,107 @@ __device__ FixOut fix_tile(const TileView& tv, uint32_t entry, const WinRec* rec
   return r;
 }
 
-// ---------------------------------------------------------------- k_walk
+// ---------------------------------------------------------------- k_cand
+// Candidate pass of one tile: inserts every position into head[] in order
+// (the table is carried in from earlier tiles) and records, per position, the
+// candidate distance that passed the first-byte check (0 = literal) and, per
+// window, its run period (WinRec::run: D when all 32 positions have distance
+// D <= 32 and equal the bytes D earlier).  Only this pass needs the head
+// table, so only it is limited to the walkers whose tables fit in shared
+// memory; the parse runs as a separate kernel with far more warps per SM.
+template <int HB>
+__device__ void cand_tile(const TileView& tv, const uint32_t* carry, uint32_t* smem_warp, uint32_t* wbuf, WinRec* rec,
+                          uint16_t* cand16) {
+  constexpr int H = 1 << HB;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1;
+  const HeadTab head{reinterpret_cast<uint16_t*>(smem_warp), reinterpret_cast<uint8_t*>(smem_warp) + 2 * H};
+  if (carry) {
+#pragma unroll 8
+    for (int i = lane; i < H; i += 32) {
+      const uint32_t pos = __ldg(carry + i);
+      head.put(i, pos, pos ? tv.sb.byte(pos) : 0u);
+    }
+  } else {
+    for (int i = lane; i < H; i += 32) head.put(i, 0, 0);
+  }
+  __syncwarp();
+  const uint32_t tend = tv.ts + tv.tl;
+  const uint32_t nwin = (tv.tl + 31) >> 5;
+  uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
+  for (uint32_t w = 0; w < nwin; ++w) {
+    const uint32_t wpos = tv.ts + (w << 5);
+    const uint32_t woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
+    if (w + 1 < nwin) pre = prefetch_window(tv.sb, wpos + 32, lane);
+    const uint32_t p = wpos + lane;
+    const bool ins = p < tend && p + 4 <= tv.n;
+    const uint32_t v4 = wload4(wbuf, woff + lane);
+    const uint32_t h = ins ? hash_fast(v4, HB) : kFull;
+    const uint32_t peers = __match_any_sync(kFull, h);
+    const uint32_t before = peers & lt;
+    const uint32_t src = before ? 31 - __clz(before) : lane;
+    const uint32_t vb = __shfl_sync(kFull, v4, src);
+    uint32_t cpos = 0, cbyte = 0;  // candidate: position mod 32768 | valid bit, first byte
+    if (ins) {
+      if (before) {
+        const uint32_t c = wpos + src;
+        cpos = c ? ((c & 0x7FFFu) | 0x8000u) : 0u;
+        cbyte = vb & 0xFFu;
+      } else {
+        cpos = head.pos[h];
+        cbyte = head.byte[h];
+      }
+    }
+    __syncwarp();
+    if (ins && (peers >> lane) == 1u) head.put(h, p, v4 & 0xFFu);
+    uint32_t d = 0;
+    if (cpos & 0x8000u) {
+      const uint32_t dist = (p - (cpos & 0x7FFFu)) & 0x7FFFu;
+      if (dist != 0 && cbyte == (v4 & 0xFFu)) d = dist;
+    }
+    if (p < tend) cand16[p - tv.ts] = uint16_t(d);
+    const uint32_t D = __shfl_sync(kFull, d, 0);
+    const bool ok = wpos >= 32 && D != 0 && D <= 32 && d == D && p + 4 <= tend && wload4(wbuf, woff + lane - D) == v4;
+    const uint32_t all = __ballot_sync(kFull, ok);
+    if (lane == 0) rec[w].run = all == kFull ? D : 0u;
+    __syncwarp();
+  }
+}
+
 template <int HB, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_walk(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
+__global__ void __launch_bounds__(WARPS * 32) k_cand(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
                                                       uint32_t* __restrict__ counter) {
   extern __shared__ uint32_t sm[];
   constexpr uint32_t HW = ((1u << HB) * 3 + 3) / 4;
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t* head = sm + wid * walker_words<HB>();
-  uint32_t* ring = head + HW;
+  uint32_t* head = sm + wid * (HW + kWbuf);
+  uint32_t* wbuf = head + HW;
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(counter, 1u);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= nlist) break;
+    const Tile t = wk.tiles[list[i]];
+    const Segment sg = wk.segs[t.seg];
+    const TileView tv = tile_view(wk, t, sg);
+    const uint32_t* carry = t.index ? reinterpret_cast<const uint32_t*>(wk.scratch + t.carry) : nullptr;
+    cand_tile<HB>(tv, carry, head, wbuf, reinterpret_cast<WinRec*>(wk.scratch + t.rec),
+                  reinterpret_cast<uint16_t*>(wk.scratch + t.cand));
+  }
+}
+
+// ---------------------------------------------------------------- k_parse
+// Speculative parse of one tile (parse entry = tile start) from the recorded
+// candidates: greedy parse, fixed-Huffman bits, and per window the parse
+// entry, bit offset and match count for the fix-up.  Windows that a match
+// covers entirely cost only that record.  Shared memory per warp is the bit
+// ring and the staged bytes, so many warps share an SM.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 3) k_parse(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
+                                                          uint32_t* __restrict__ counter) {
+  __shared__ uint32_t sm[WARPS][kRing + kWbuf];
+  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* ring = sm[wid];
   uint32_t* wbuf = ring + kRing;
   for (;;) {
     uint32_t i = 0;
@@ -471,20 +568,51 @@ __global__ void __launch_bounds__(WARPS * 32) k_walk(Work wk, const uint32_t* __
     const Tile t = *tp;
     const Segment sg = wk.segs[t.seg];
     const TileView tv = tile_view(wk, t, sg);
-    const uint32_t* carry = t.index ? reinterpret_cast<const uint32_t*>(wk.scratch + t.carry) : nullptr;
-    WinRec* rec = t.index ? reinterpret_cast<WinRec*>(wk.scratch + t.rec) : nullptr;
-    uint16_t* c16 = t.index ? reinterpret_cast<uint16_t*>(wk.scratch + t.cand) : nullptr;
+    WinRec* rec = reinterpret_cast<WinRec*>(wk.scratch + t.rec);
+    const uint16_t* c16 = reinterpret_cast<const uint16_t*>(wk.scratch + t.cand);
     uint32_t* out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch);
-    const WinState r = walk_tile<HB>(tv, carry, head, ring, wbuf, out, rec, c16);
+    for (uint32_t k = lane; k < kRing; k += 32) ring[k] = 0;
+    __syncwarp();
+    WinState st{tv.ts, 0, 0, 0, 0};
+    const uint32_t tend = tv.ts + tv.tl;
+    const uint32_t nwin = (tv.tl + 31) >> 5;
+    // the next window's bytes and candidates are loaded one window ahead
+    uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
+    uint32_t dnext = lane < tv.tl ? c16[lane] : 0u;
+    uint32_t pre_w = 0;
+    for (uint32_t w = 0; w < nwin; ++w) {
+      const uint32_t wpos = tv.ts + (w << 5);
+      const uint32_t lim = min(32u, tend - wpos);
+      // parse state where the parse enters this window (lanes 0-2 write one field each)
+      const uint32_t f = lane == 0 ? st.np - tv.ts : lane == 1 ? st.cursor : st.matches;
+      if (lane < 3) reinterpret_cast<uint32_t*>(rec + w)[lane] = f;
+      if (st.np >= wpos + lim) continue;  // covered by a match
+      uint32_t woff, d;
+      if (pre_w == w) {
+        woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
+        d = dnext;
+      } else {
+        woff = stage_window(tv.sb, wpos, wbuf, lane, prefetch_window(tv.sb, wpos, lane));
+        d = lane < lim ? c16[(w << 5) + lane] : 0u;
+      }
+      if (w + 1 < nwin) {
+        pre = prefetch_window(tv.sb, wpos + 32, lane);
+        const uint32_t q = ((w + 1) << 5) + lane;
+        dnext = q < tv.tl ? c16[q] : 0u;
+        pre_w = w + 1;
+      }
+      parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st);
+    }
+    flush_tail(ring, out, st, lane);
     if (lane == 0) {
-      tp->spec_bits = r.cursor;
-      tp->spec_matches = r.matches;
-      tp->spec_exit = r.np;
-      tp->spec_tokens = r.tokens;
+      tp->spec_bits = st.cursor;
+      tp->spec_matches = st.matches;
+      tp->spec_exit = st.np;
+      tp->spec_tokens = st.tokens;
       tp->fix_bits = 0;
       tp->splice_bit = 0;
-      tp->fin_matches = r.matches;
-      tp->fin_exit = r.np;
+      tp->fin_matches = st.matches;
+      tp->fin_exit = st.np;
       tp->fix_entry = t.start;
     }
   }
@@ -587,17 +715,18 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
   // bits), and one CTA of 17 (219 KB) holds one more per SM than four CTAs
   // of four, since every CTA also reserves 1 KB; 5% faster.  At 14 hash bits
   // (49.7 KB each) four fit either way.
-  constexpr int WARPS = HB <= 12 ? 17 : 1;
+  constexpr int WARPS = HB <= 12 ? 18 : 4;
   const size_t tbl_bytes = size_t(H) * 4;
-  const size_t wsm = size_t(WARPS) * walker_words<HB>() * 4;
+  constexpr uint32_t HW = ((1u << HB) * 3 + 3) / 4;
+  const size_t csm = size_t(WARPS) * (HW + kWbuf) * 4;  // head table + staged bytes per walker
   // walker CTAs per SM, and the kernels' shared-memory limits, once per device
   static std::atomic<int> walk_per_sm[64];
   const int ds = device_slot();
   int per_sm = walk_per_sm[ds].load(std::memory_order_relaxed);
   if (!per_sm) {
     cudaFuncSetAttribute(k_lastocc<HB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tbl_bytes));
-    cudaFuncSetAttribute(k_walk<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<HB, WARPS>, WARPS * 32, wsm);
+    cudaFuncSetAttribute(k_cand<HB, WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(csm));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cand<HB, WARPS>, WARPS * 32, csm);
     if (per_sm < 1) per_sm = 1;
     walk_per_sm[ds].store(per_sm, std::memory_order_relaxed);
   }
@@ -611,7 +740,20 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
     uint32_t blocks = uint32_t(per_sm) * uint32_t(sms);
     const uint32_t need = (L.n_walk + WARPS - 1) / WARPS;
     if (blocks > need) blocks = need;
-    k_walk<HB, WARPS><<<blocks, WARPS * 32, wsm, st>>>(wk, L.walk, L.n_walk, L.counter);
+    k_cand<HB, WARPS><<<blocks, WARPS * 32, csm, st>>>(wk, L.walk, L.n_walk, L.counter);
+    mk->mark(kPhCand, st);
+    constexpr int PW = 16;
+    static std::atomic<int> parse_per_sm[64];
+    int pps = parse_per_sm[ds].load(std::memory_order_relaxed);
+    if (!pps) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pps, k_parse<PW>, PW * 32, 0);
+      if (pps < 1) pps = 1;
+      parse_per_sm[ds].store(pps, std::memory_order_relaxed);
+    }
+    uint32_t pblocks = uint32_t(sms) * uint32_t(pps);
+    const uint32_t pneed = (L.n_walk + PW - 1) / PW;
+    if (pblocks > pneed) pblocks = pneed;
+    k_parse<PW><<<pblocks, PW * 32, 0, st>>>(wk, L.walk, L.n_walk, L.counter + 6);
   }
   mk->mark(kPhWalk, st);
   if (L.n_multi) {
