@@ -69,16 +69,20 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# Many host threads call the engine at once in some legs (each call on its own
+# CUDA stream): let the device run that many streams' work side by side
+# instead of the default 8 hardware queues.  Must be set before CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "deflate_compress_GBps_batched"
 UNIT = "GB/s"
 WORKLOAD = "10000 zlib buffers, log-uniform 1 KiB-4 MiB, mixed text/ints/zeros/random, level 1, one pass"
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per input byte of the walk kernel, measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on the first 600 buffers of
-# this workload (301.5 MB): 602 MB + 850 MB.  Every term of that traffic is per
-# byte or per tile, so it is scaled by the input size for the full launch.
-WALK_DRAM_BYTES_PER_INPUT_BYTE = (602.359296e6 + 850.131200e6) / 301540590
+# DRAM bytes (read + write) per input byte of the dominant kernel, from one
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) on a slice of
+# this workload; every term of that traffic is per byte or per tile, so it is
+# scaled by the input size for the full launch.  Empty until measured.
+DRAM_BYTES_PER_INPUT_BYTE = {}
 
 
 def parse():
@@ -459,8 +463,8 @@ def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
 # ---------------------------------------------------------------- the other configurations
 # ncu figures of the two dominant kernels (profiles/): warp instructions per
 # input byte, for the issue-rate roofline (4 warp instructions per SM cycle).
-WARP_INST_PER_BYTE = {"walk": 10.5, "lazy_match": 89.0}
-PHASE_KERNEL = {"walk": "k_walk", "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
+WARP_INST_PER_BYTE = {"lazy_match": 89.0}
+PHASE_KERNEL = {"candidates": "k_cand", "parse": "k_parse", "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
                 "hash_carry": "k_lastocc + k_carry_scan", "fixup": "k_fix1 + k_fix2", "join": "k_join",
                 "checksum": "k_ck_block + k_ck_fold", "plan": "k_plan + k_zero"}
 
@@ -624,7 +628,10 @@ def measure_threads(deflate, buf, sizes, offs, level, threads, sample_bytes):
         return int(r)
 
     with cf.ThreadPoolExecutor(threads) as ex:
-        list(ex.map(one, idx[:threads * 4]))  # warm every engine
+        # warm every engine: its arenas grow to the largest buffers once
+        biggest = sorted(idx, key=lambda i: -sizes[i])[:threads * 4]
+        list(ex.map(one, biggest))
+        list(ex.map(one, idx[:threads * 8]))
         t0 = time.perf_counter()
         outs = list(ex.map(one, idx))
         dt = time.perf_counter() - t0
@@ -735,8 +742,9 @@ def main():
     clocks = clk.summary()
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     roofline = roofline_of(phases, total, comp, clocks.get("sm_mhz"), sms)
-    roofline["traffic"] = WALK_DRAM_BYTES_PER_INPUT_BYTE * total if roofline["dominant_phase"] == "walk" else None
-    roofline["traffic_note"] = "ncu DRAM bytes per input byte of the walk kernel on a 301.5 MB slice, scaled"
+    tb = DRAM_BYTES_PER_INPUT_BYTE.get(roofline["dominant_phase"])
+    roofline["traffic"] = tb * total if tb else None
+    roofline["traffic_note"] = "ncu DRAM bytes per input byte of the dominant kernel on a slice of the workload, scaled"
     b.close()
 
     # -- plain path: one pass per buffer (device-resident) and deflate_compress per buffer

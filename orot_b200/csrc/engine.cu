@@ -47,6 +47,9 @@ bool DevBuf::ensure(size_t n) {
   if (n <= cap) return true;
   size_t want = std::max(n, cap + cap / 2);  // grow geometrically
   if (pool) {
+    // pool arenas double (at least 1 MiB): mapping new memory into the pool
+    // is the slow part of an allocation, so it should happen rarely
+    want = std::max({n, 2 * cap, size_t(1) << 20});
     if (p) cudaFreeAsync(p, st);
     p = nullptr;
     cap = 0;

@@ -17,7 +17,7 @@
 //                 insert; the candidate distance of every position (2 bytes)
 //                 and the run period of every 32-position window.
 //   k_parse       one warp per tile, no table (16 warps of 0.6 KB per CTA,
-//                 many CTAs per SM): capped match lengths per lane, greedy
+//                 two CTAs per SM): capped match lengths per lane, greedy
 //                 parse resolved with ballots, fixed Huffman bits packed with
 //                 shared atomics and flushed as coalesced 128-byte stores.
 //                 The parse starts at the tile's first byte (speculation) and
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_cand(Work wk, const uint32_t* __
 // covers entirely cost only that record.  Shared memory per warp is the bit
 // ring and the staged bytes, so many warps share an SM.
 template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 3) k_parse(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
+__global__ void __launch_bounds__(WARPS * 32, 2) k_parse(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
                                                           uint32_t* __restrict__ counter) {
   __shared__ uint32_t sm[WARPS][kRing + kWbuf];
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;

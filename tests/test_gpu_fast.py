@@ -170,10 +170,11 @@ def test_device_batch_equals_single_calls(gpu):
 def test_launch_count_matches_the_kernels_of_a_pass(gpu):
     """deflate_gpu_batch_launches counts every kernel of a pass: at level 1
     with a multi-tile buffer and zlib framing that is k_lastocc, k_carry_scan,
-    k_walk, k_fix1, k_fix2, k_plan, k_zero, k_join, k_ck_block, k_ck_fold and
-    k_frame (11); raw output drops the two checksum kernels."""
+    k_cand, k_parse, k_fix1, k_fix2, k_plan_seg, k_plan_stream,
+    k_plan_pieces, k_zero, k_join, k_ck_block, k_ck_fold and k_frame (14);
+    raw output drops the two checksum kernels."""
     d = synth.gen(3 << 20, synth.MIXED, 2)
-    for fmt, want in ((gpu.Format.Zlib, 11), (gpu.Format.Raw, 9)):
+    for fmt, want in ((gpu.Format.Zlib, 14), (gpu.Format.Raw, 12)):
         b = gpu.DeviceBatch()
         b.load(d, [len(d)], 1, fmt)
         b.run()
