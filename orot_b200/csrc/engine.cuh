@@ -23,7 +23,6 @@ constexpr int kBlkStored = 0, kBlkFixed = 1, kBlkDynamic = 2;
 // Segment flags.
 constexpr uint32_t kSegLast = 1u;        // BFINAL block of its stream
 constexpr uint32_t kSegWholeBuf = 2u;    // whole-buffer rule: all-literal parse -> stored
-constexpr uint32_t kSegFullSearch = 4u;  // levels 4-9: search every position with the full chain
 
 // Stream error codes written to Stream::error.
 constexpr uint32_t kErrNone = 0, kErrCapacity = 1, kErrInternal = 2;

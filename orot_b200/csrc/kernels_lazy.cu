@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
       uint32_t* sx = scan;  // where each segment's parse leaves it
       const uint32_t S = (tl + 31) / 32;
       const uint32_t nsearch = tl >= 4 ? tl - 3 : 0;
-      const bool refine = !cfg.opt && cfg.chain > kChain0 && !(sg.flags & kSegFullSearch);
+      const bool refine = !cfg.opt && cfg.chain > kChain0;
       for (uint32_t i = nsearch + tid; i < kFmWords * 32; i += blockDim.x) F[i] = 0;
       for (uint32_t w = tid; w < kFmWords; w += blockDim.x) fullm[w] = refine ? 0u : kAll;
       if (tid == 0) scan[62] = 0;

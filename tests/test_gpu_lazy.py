@@ -113,25 +113,3 @@ def test_lazy_window_runs_match_single_tiles(gpu, oracle, level, monkeypatch):
         assert zlib.decompress(out) == d
     ref = oracle.compress(bufs[1], level, 1)
     assert within(len(outs["16"][1]), len(ref)), (len(outs["16"][1]), len(ref))
-
-
-@pytest.mark.parametrize("level", [4, 6, 9])
-def test_refined_search_equals_full_search(gpu, level, monkeypatch):
-    """Levels 4-9 search fully only where the lazy parse reads and repeat the
-    parse until it reads only full results; the tokens then equal those of a
-    full search at every position (OROT_B200_FULL_SEARCH=1)."""
-    sizes = [3 << 20, 1 << 20, 700001, 4128 * 5 + 17, 100]
-    kinds = [synth.MIXED, synth.TEXT, synth.PERIODIC, synth.INTS, synth.ZEROS]
-    bufs = [synth.gen(n, k, 70 + i) for i, (n, k) in enumerate(zip(sizes, kinds))]
-    outs = {}
-    for full in ("0", "1"):
-        monkeypatch.setenv("OROT_B200_FULL_SEARCH", full)
-        b = gpu.DeviceBatch()
-        b.load(b"".join(bufs), sizes, level, gpu.Format.Raw)
-        b.run()
-        got = b.sizes()
-        outs[full] = [b.output(i, got[i]) for i in range(len(sizes))]
-        b.close()
-    for d, o in zip(bufs, outs["0"]):
-        assert zlib.decompress(o, -15) == d
-    assert outs["0"] == outs["1"]
