@@ -78,7 +78,9 @@ struct WinRec {
   uint32_t bit;        // bit offset of that token in the tile's stream
   uint32_t matches;    // match tokens before it
   uint32_t run;        // D when all 32 positions have candidate distance D <= 32
-                       // and equal the bytes D earlier (a run window), else 0
+                       // and equal the bytes D earlier (a run window), else 0;
+                       // in the fast-level kernels' records, bits 8.. hold the
+                       // first window after the run
 };
 
 struct Tile {

@@ -160,16 +160,21 @@ __device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_
   const uint32_t qa = q + sb.boff;
   const uint32_t* qw = sb.w + (qa >> 2);
   const uint32_t qs = (qa & 3) * 8;
+  const uint32_t* pw = wbuf + (po >> 2);  // p side: staged words, each loaded once
+  const uint32_t ps = (po & 3) * 8;
   uint32_t v[PRE];
 #pragma unroll
   for (int j = 0; j < PRE; ++j) v[j] = active && uint32_t(j) * 4 < cap + 4 ? __ldg(qw + j) : 0u;
   uint32_t n = 0;
   bool open = active && cap > 0;
+  uint32_t plo = pw[0];
 #pragma unroll
   for (int j = 0; j < PRE - 1; ++j) {
     if (!__any_sync(kFull, open)) break;
     if (open) {
-      const uint32_t x = wload4(wbuf, po + 4 * j) ^ __funnelshift_r(v[j], v[j + 1], qs);
+      const uint32_t phi = pw[j + 1];
+      const uint32_t x = __funnelshift_r(plo, phi, ps) ^ __funnelshift_r(v[j], v[j + 1], qs);
+      plo = phi;
       if (x) { n += (__ffs(x) - 1) >> 3; open = false; } else { n += 4; }
       if (n >= cap) open = false;
     }
@@ -178,13 +183,46 @@ __device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_
   for (uint32_t j = PRE - 1; __any_sync(kFull, open); ++j) {
     if (open) {
       const uint32_t hi = __ldg(qw + j + 1);
-      const uint32_t x = wload4(wbuf, po + 4 * j) ^ __funnelshift_r(lo, hi, qs);
+      const uint32_t phi = pw[j + 1];
+      const uint32_t x = __funnelshift_r(plo, phi, ps) ^ __funnelshift_r(lo, hi, qs);
+      plo = phi;
       lo = hi;
       if (x) { n += (__ffs(x) - 1) >> 3; open = false; } else { n += 4; }
       if (n >= cap) open = false;
     }
   }
   return n < cap ? n : cap;
+}
+
+// Fixed-Huffman code tables for the parse kernels: literal b at [b], match
+// length L (3..258) at [256 + L]; each entry is the LSB-first bits | count << 16
+// (a length entry holds the length symbol and its extra bits).
+constexpr uint32_t kCodeTab = 256 + 259;
+__device__ __forceinline__ void fill_code_tab(uint32_t* tab) {
+  for (uint32_t i = threadIdx.x; i < kCodeTab; i += blockDim.x) {
+    uint32_t bits = 0, nb = 0;
+    if (i < 256) {
+      fixed_literal(i, bits, nb);
+    } else if (i >= 256 + 3) {
+      uint32_t li, le, lv;
+      length_code(i - 256, li, le, lv);
+      const uint32_t sym = 257 + li;
+      const uint32_t c = sym <= 279 ? sym - 256 : 0xC0u + (sym - 280), cl = sym <= 279 ? 7u : 8u;
+      bits = rev_bits(c, cl) | (lv << cl);
+      nb = cl + le;
+    }
+    tab[i] = bits | (nb << 16);
+  }
+}
+__device__ __forceinline__ void tab_match(const uint32_t* tab, uint32_t len, uint32_t dist, uint32_t& bits,
+                                          uint32_t& nb) {
+  const uint32_t t = tab[256 + len];
+  uint32_t dc, de, dv;
+  dist_code(dist, dc, de, dv);
+  bits = (t & 0xFFFFu) | (rev_bits(dc, 5) << (t >> 16));
+  nb = (t >> 16) + 5;
+  bits |= dv << nb;
+  nb += de;
 }
 
 // head[] entry: the candidate's position mod 32768 with a valid bit (u16)
@@ -209,7 +247,8 @@ __host__ __device__ constexpr uint32_t walker_words() { return ((1u << HB) * 3 +
 // `lane` holds position wpos+lane; `d` is its candidate distance (0 = none).
 __device__ __forceinline__ void parse_window(const SegBytes& sb, uint32_t n, uint32_t wpos, uint32_t lim,
                                              uint32_t lane, const uint32_t* wbuf, uint32_t woff, uint32_t d,
-                                             uint32_t* ring, uint32_t* out, WinState& st) {
+                                             uint32_t* ring, uint32_t* out, WinState& st,
+                                             const uint32_t* ctab = nullptr) {
   const uint32_t p = wpos + lane;
   uint32_t clen = 0;
   bool exact = true;
@@ -265,8 +304,19 @@ __device__ __forceinline__ void parse_window(const SegBytes& sb, uint32_t n, uin
   const bool ism = vis && ((M >> lane) & 1u);
   uint32_t code = 0, nb = 0;
   if (vis) {
-    if (ism) fixed_match(int(lane) == xl ? full : clen, d, code, nb);
-    else fixed_literal(wload4(wbuf, woff + lane) & 0xFFu, code, nb);
+    if (ctab) {
+      if (ism) {
+        tab_match(ctab, int(lane) == xl ? full : clen, d, code, nb);
+      } else {
+        const uint32_t t = ctab[wload4(wbuf, woff + lane) & 0xFFu];
+        code = t & 0xFFFFu;
+        nb = t >> 16;
+      }
+    } else if (ism) {
+      fixed_match(int(lane) == xl ? full : clen, d, code, nb);
+    } else {
+      fixed_literal(wload4(wbuf, woff + lane) & 0xFFu, code, nb);
+    }
   }
   uint32_t incl = nb;
 #pragma unroll
@@ -409,14 +459,9 @@ __device__ FixOut fix_tile(const TileView& tv, uint32_t entry, const WinRec* rec
     const uint32_t lim = min(32u, tend - wpos);
     if (st.np >= wpos + lim) continue;
     if (rc.run) {
-      // extent of the run: windows w.. with the same period
-      const uint32_t D = rc.run;
-      uint32_t wend = nwin;
-      for (uint32_t b = w + 1; b < nwin; b += 32) {
-        const bool stop = b + lane < nwin && rec[b + lane].run != D;
-        const uint32_t m = __ballot_sync(kFull, stop);
-        if (m) { wend = b + __ffs(m) - 1; break; }
-      }
+      // the run's period and the first window after it (recorded by k_cand)
+      const uint32_t D = rc.run & 0xFFu;
+      const uint32_t wend = rc.run >> 8;
       const uint32_t rend = tv.ts + (wend << 5);  // bytes before rend all repeat at distance D
       if (st.np + 258 <= rend) {
         const uint32_t k = (rend - st.np) / 258;
@@ -462,7 +507,8 @@ __device__ FixOut fix_tile(const TileView& tv, uint32_t entry, const WinRec* rec
 // (the table is carried in from earlier tiles) and records, per position, the
 // candidate distance that passed the first-byte check (0 = literal) and, per
 // window, its run period (WinRec::run: D when all 32 positions have distance
-// D <= 32 and equal the bytes D earlier).  Only this pass needs the head
+// D <= 32 and equal the bytes D earlier, with the first window after the run
+// in bits 8 and up; 0 for other windows).  Only this pass needs the head
 // table, so only it is limited to the walkers whose tables fit in shared
 // memory; the parse runs as a separate kernel with far more warps per SM.
 template <int HB>
@@ -484,6 +530,7 @@ __device__ void cand_tile(const TileView& tv, const uint32_t* carry, uint32_t* s
   __syncwarp();
   const uint32_t tend = tv.ts + tv.tl;
   const uint32_t nwin = (tv.tl + 31) >> 5;
+  uint32_t seg_D = 0, seg_start = 0;  // the run being recorded: its period and first window
   uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
   for (uint32_t w = 0; w < nwin; ++w) {
     const uint32_t wpos = tv.ts + (w << 5);
@@ -518,10 +565,21 @@ __device__ void cand_tile(const TileView& tv, const uint32_t* carry, uint32_t* s
     if (p < tend) cand16[p - tv.ts] = uint16_t(d);
     const uint32_t D = __shfl_sync(kFull, d, 0);
     const bool ok = wpos >= 32 && D != 0 && D <= 32 && d == D && p + 4 <= tend && wload4(wbuf, woff + lane - D) == v4;
-    const uint32_t all = __ballot_sync(kFull, ok);
-    if (lane == 0) rec[w].run = all == kFull ? D : 0u;
+    const uint32_t runD = __ballot_sync(kFull, ok) == kFull ? D : 0u;
+    // consecutive run windows of one period form a run; when it ends, each of
+    // its windows records the period and the window after the run, so the
+    // fix-up crosses a run without scanning it
+    if (runD != seg_D) {
+      if (seg_D)
+        for (uint32_t k = seg_start + lane; k < w; k += 32) rec[k].run = seg_D | (w << 8);
+      seg_D = runD;
+      seg_start = w;
+    }
+    if (!runD && lane == 0) rec[w].run = 0;
     __syncwarp();
   }
+  if (seg_D)
+    for (uint32_t k = seg_start + lane; k < nwin; k += 32) rec[k].run = seg_D | (nwin << 8);
 }
 
 template <int HB, int WARPS>
@@ -556,9 +614,12 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 2) k_parse(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
                                                           uint32_t* __restrict__ counter) {
   __shared__ uint32_t sm[WARPS][kRing + kWbuf];
+  __shared__ uint32_t ctab[kCodeTab];
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* ring = sm[wid];
   uint32_t* wbuf = ring + kRing;
+  fill_code_tab(ctab);
+  __syncthreads();
   for (;;) {
     uint32_t i = 0;
     if (lane == 0) i = atomicAdd(counter, 1u);
@@ -601,7 +662,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_parse(Work wk, const uint32_t
         dnext = q < tv.tl ? c16[q] : 0u;
         pre_w = w + 1;
       }
-      parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st);
+      parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st, ctab);
     }
     flush_tail(ring, out, st, lane);
     if (lane == 0) {

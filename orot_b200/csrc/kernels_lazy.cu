@@ -630,8 +630,8 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
 }
 
 // ---------------------------------------------------------------- Huffman
-// Code lengths for one alphabet, single thread.  Symbols with non-zero
-// frequency are sorted by (frequency, symbol); the two-queue construction
+// Code lengths for one alphabet.  Symbols with non-zero frequency are sorted
+// by (frequency, symbol) (by the warp, huff_sort); on one thread the two-queue construction
 // (leaves in sorted order, internal nodes in creation order, a leaf wins a
 // tie) builds an optimal tree; if it is deeper than `limit` the per-length
 // counts are adjusted as in ITU-T T.81 Annex K.3 and lengths are handed out
@@ -644,21 +644,35 @@ struct HuffScratch {
   uint32_t cnt[64];
 };
 
-__device__ void huff_lengths(const uint32_t* freq, int n, uint8_t* len, int limit, HuffScratch& s) {
+// Sorts the used symbols (non-zero frequency) by (frequency, symbol) into
+// s.sym and clears len[]: every lane ranks its symbols against all others.
+// All lanes of the warp call it; returns the number of used symbols.
+__device__ int huff_sort(const uint32_t* freq, int n, uint8_t* len, HuffScratch& s) {
+  const int lane = int(threadIdx.x & 31);
   int m = 0;
-  for (int i = 0; i < n; ++i) {
-    len[i] = 0;
-    if (freq[i]) s.sym[m++] = uint16_t(i);
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    const int i = i0 + lane;
+    m += __popc(__ballot_sync(kAll, i < n && freq[i] != 0));
+    if (i < n) len[i] = 0;
   }
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t fi = freq[i];
+    if (!fi) continue;
+    int r = 0;
+    for (int j = 0; j < n; ++j) {
+      const uint32_t fj = freq[j];
+      r += (fj != 0 && (fj < fi || (fj == fi && j < i))) ? 1 : 0;
+    }
+    s.sym[r] = uint16_t(i);
+  }
+  __syncwarp();
+  return m;
+}
+
+// Code lengths of the m sorted symbols (one lane; after huff_sort).
+__device__ void huff_lengths(const uint32_t* freq, int m, uint8_t* len, int limit, HuffScratch& s) {
   if (m == 0) return;
   if (m == 1) { len[s.sym[0]] = 1; return; }
-  for (int i = 1; i < m; ++i) {  // insertion sort by (freq, symbol)
-    const uint16_t x = s.sym[i];
-    const uint32_t fx = freq[x];
-    int j = i - 1;
-    while (j >= 0 && freq[s.sym[j]] > fx) { s.sym[j + 1] = s.sym[j]; --j; }
-    s.sym[j + 1] = x;
-  }
   int li = 0, ni = 0;
   for (int k = 0; k < m - 1; ++k) {
     uint32_t wsum = 0;
@@ -765,15 +779,26 @@ __global__ void __launch_bounds__(kHuffWarps * 32) k_huff(Work wk, const uint32_
   uint32_t* codes = reinterpret_cast<uint32_t*>(wk.scratch + sg.codes);
   uint32_t* hdr = reinterpret_cast<uint32_t*>(wk.scratch + sg.hdr_off);
   for (uint32_t i = lane; i < 256; i += 32) hdr[i] = 0;
+  if (lane == 0) H.freq[256] = 1;  // EOB
   __syncwarp();
+  const bool all_literal = (sg.flags & kSegWholeBuf) && mt == 0;  // warp-uniform
+  int m_ll = 0, m_dl = 0;
+  if (!all_literal) {
+    // the symbol sorts of both alphabets, by the whole warp
+    m_ll = huff_sort(H.freq, 288, H.ll, H.hs);
+    if (lane == 0) huff_lengths(H.freq, m_ll, H.ll, 15, H.hs);
+    __syncwarp();
+    m_dl = huff_sort(H.freq + 288, 32, H.dl, H.hs);
+    if (lane == 0) huff_lengths(H.freq + 288, m_dl, H.dl, 15, H.hs);
+    __syncwarp();
+  }
   if (lane != 0) return;
 
-  H.freq[256] = 1;  // EOB
   uint32_t type;
   uint32_t hbits = 0, eob = 0;
   const uint32_t pieces = sg.len ? (sg.len + 65534) / 65535 : 1;
   const uint64_t stored_bits = (uint64_t(sg.len) + 5ull * pieces) * 8;
-  if ((sg.flags & kSegWholeBuf) && mt == 0) {
+  if (all_literal) {
     type = kBlkStored;  // all-literal parse (block_compressor.cpp:60-61)
   } else {
     // fixed cost (deflate_block.cpp:50-70)
@@ -783,9 +808,8 @@ __global__ void __launch_bounds__(kHuffWarps * 32) k_huff(Work wk, const uint32_
     uint64_t fixed_bits = 3 + ext;
     for (int i = 0; i < 288; ++i) fixed_bits += uint64_t(i < 144 ? 8 : i < 256 ? 9 : i < 280 ? 7 : 8) * H.freq[i];
     for (int i = 0; i < 30; ++i) fixed_bits += 5ull * H.freq[288 + i];
-    // dynamic code (deflate_block.cpp:347-383 conventions)
-    huff_lengths(H.freq, 288, H.ll, 15, H.hs);
-    huff_lengths(H.freq + 288, 32, H.dl, 15, H.hs);
+    // dynamic code (deflate_block.cpp:347-383 conventions); the lengths of
+    // both alphabets were built above
     if (H.ll[256] == 0) H.ll[256] = 1;
     bool any = false;
     for (int i = 0; i < 32; ++i) any |= H.dl[i] != 0;
@@ -819,7 +843,15 @@ __global__ void __launch_bounds__(kHuffWarps * 32) k_huff(Work wk, const uint32_
     }
     for (int i = 0; i < 19; ++i) H.clf[i] = 0;
     for (int i = 0; i < nr; ++i) ++H.clf[H.rsym[i]];
-    huff_lengths(H.clf, 19, H.cl, 7, H.hs);
+    int m_cl = 0;
+    for (int i = 0; i < 19; ++i) {  // 19 symbols: sorted on this lane (insertion by (frequency, symbol))
+      H.cl[i] = 0;
+      if (!H.clf[i]) continue;
+      int j = m_cl++;
+      while (j > 0 && H.clf[H.hs.sym[j - 1]] > H.clf[i]) { H.hs.sym[j] = H.hs.sym[j - 1]; --j; }
+      H.hs.sym[j] = uint16_t(i);
+    }
+    huff_lengths(H.clf, m_cl, H.cl, 7, H.hs);
     canon(H.cl, 19, H.clc);
     int hclen = 19;
     while (hclen > 4 && H.cl[c_cl_order[hclen - 1]] == 0) --hclen;
