@@ -102,6 +102,7 @@ __global__ void k_plan_stream(Work wk) {
   const bool bare = (s.mode & kStreamBare) != 0;
   const uint32_t hdr = bare ? 0 : fmt_header_bytes(s.fmt), trl = bare ? 0 : fmt_trailer_bytes(s.fmt);
   uint64_t c = 0;  // bits from the start of the raw DEFLATE stream
+  bool fault = false;  // a kernel could not finish one of the stream's segments
   for (uint32_t g0 = s.seg_first; g0 < s.seg_first + s.seg_count; g0 += 32) {
     const uint32_t cnt = min(32u, s.seg_first + s.seg_count - g0);
     uint32_t type = 0, len = 0, last = 0;
@@ -112,6 +113,7 @@ __global__ void k_plan_stream(Work wk) {
       len = sg.len;
       last = sg.flags & kSegLast;
       bits = sg.bits;
+      if (sg.flags & kSegFault) fault = true;
     }
     uint64_t my_off = 0, my_bits = 0;
     for (uint32_t j = 0; j < cnt; ++j) {
@@ -128,13 +130,14 @@ __global__ void k_plan_stream(Work wk) {
       wk.segs[g0 + lane].bits = my_bits;
     }
   }
+  fault = __any_sync(kFullMask, fault);
   if (lane) return;
   Piece* tail = wk.pieces + s.piece_first + s.piece_count - 2;  // the open part's sync point
   const uint64_t sync_at = c;
   if (s.mode & kStreamOpen) c = ((c + 3 + 7) & ~uint64_t(7)) + 32;  // empty stored block, BFINAL = 0
   const uint64_t size = uint64_t(hdr) + c / 8 + trl;
   s.raw_bits = c;
-  s.error = size > s.out_cap ? kErrCapacity : kErrNone;
+  s.error = fault ? kErrInternal : size > s.out_cap ? kErrCapacity : kErrNone;
   s.out_size = s.error ? 0 : size;
   if (s.mode & kStreamOpen) {
     uint32_t* dst = reinterpret_cast<uint32_t*>(wk.out + s.out_off);

@@ -64,6 +64,7 @@ static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words 
 static_assert((kRegion + 31) / 32 * 8 <= kFBytes, "first/last marks of every link chunk fit F");
 
 constexpr uint32_t kSerialParse = 128;  // at most this many match positions: serial parse
+constexpr int kStepsPerRound = 4;       // chain steps a searching lane takes between re-balancing rounds
 
 // chain, nice, lazy depth, miss limit, optimal parse (levels 10-12)
 struct LazyCfg { int chain, nice, lazy, miss, opt; };
@@ -99,6 +100,7 @@ __device__ __forceinline__ uint32_t hash15(uint32_t v) { return (v * 0x9E3779B1u
 // its next position as soon as its chain ends.
 struct LzState {
   uint32_t r, v4p, h16p, q, maxm, best, bd;
+  uint32_t pqr;  // the 4 bytes of r ending at byte `best` (the quick reject's p side), once best >= 4
   int steps, miss, bud;
 };
 
@@ -110,6 +112,7 @@ __device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, uint32
   s.maxm = maxm;
   s.best = 2;
   s.bd = 0;
+  s.pqr = 0;
   s.steps = chain;
   s.miss = 0;
   s.bud = 2 * chain + 64;  // bounds the filtered candidates too
@@ -132,7 +135,7 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
   // quick reject (src/deflate/lz77.cpp:137-142), on the 4 bytes ending at
   // byte `best`: a longer match needs all of them
   const uint32_t maxm = s.maxm, mb = s.best;
-  if (mb >= 4 && mb < maxm && sd.load4(q + mb - 3) != sd.load4(r + mb - 3)) return false;
+  if (mb >= 4 && mb < maxm && sd.load4(q + mb - 3) != s.pqr) return false;
   uint32_t len = 4;
   while (len < maxm) {
     const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
@@ -144,6 +147,7 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
     s.best = len;
     s.bd = r - q;
     if (int(len) >= nice || len >= maxm) return true;
+    if (len >= 4) s.pqr = sd.load4(r + len - 3);
   }
   return false;
 }
@@ -262,6 +266,51 @@ __device__ __forceinline__ uint16_t sym_cost(uint32_t count, uint32_t total) {
   return uint16_t(16.0f * fminf(fmaxf(b, 1.0f), 15.0f) + 0.5f);
 }
 
+// -- staging by the bulk-copy engine (TMA, untiled; the source is this GPU's
+// own input arena, no multicast): one thread starts the copy of a tile's
+// window into shared memory and the CTA waits on an mbarrier for its bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Orders this thread's earlier generic-proxy accesses to shared memory before
+// later bulk-copy writes (every thread that touched the staged bytes runs it
+// before the barrier that precedes the next copy).
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the mbarrier's phase; gives up (false) after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, phase)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_try_wait(bar, phase))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
+}
+constexpr uint64_t kStageWaitNs = 1000000000ull;  // a copy of 37 KB that takes a second has failed
+
 }  // namespace
 
 // ---------------------------------------------------------------- k_lz
@@ -285,6 +334,10 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
   if (blockIdx.x >= nruns) return;
+  __shared__ __align__(8) uint64_t stage_bar;  // completion of the bulk copy of a tile's window
+  if (tid == 0) mbar_init(&stage_bar, 1);
+  __syncthreads();
+  uint32_t stage_phase = 0;
   const uint32_t first = runs[2 * blockIdx.x];
   const uint32_t last = first + runs[2 * blockIdx.x + 1];
   const Segment sg = wk.segs[wk.tiles[first].seg];
@@ -302,10 +355,12 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     const uint64_t g0 = (sg.in_off + rs) & ~uint64_t(15);
     const uint32_t boff = uint32_t(sg.in_off + rs - g0);
     const uint32_t n16 = (boff + (copy_end - rs) + 15) / 16;
-    const uint4* src = reinterpret_cast<const uint4*>(wk.in + g0);
+    // one thread starts the bulk copy; meanwhile the CTA clears the tail (the
+    // bytes past the copy that whole-word reads may touch) and slides the
+    // links and the table, which do not depend on the new bytes
     uint4* dst = reinterpret_cast<uint4*>(sm);
-    for (uint32_t i = tid; i < kDataBytes / 16; i += blockDim.x)
-      dst[i] = i < n16 ? __ldg(src + i) : make_uint4(0, 0, 0, 0);
+    if (tid == 0) bulk_stage(dst, wk.in + g0, n16 * 16, &stage_bar);
+    for (uint32_t i = n16 + tid; i < kDataBytes / 16; i += blockDim.x) dst[i] = make_uint4(0, 0, 0, 0);
     for (uint32_t i = tid; i < 320; i += blockDim.x) hist[i] = 0;
     // -- carry links and table from the previous tile, or start empty
     uint32_t lstart = 0;
@@ -340,7 +395,15 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
       }
       lstart = keep;
     }
-    __syncthreads();
+    const bool staged = mbar_wait(&stage_bar, stage_phase, kStageWaitNs);
+    stage_phase ^= 1u;
+    if (!__syncthreads_and(staged)) {
+      // the copy did not complete: mark the stream failed, give the copy
+      // another bounded wait so that no copy is left in flight, and stop
+      if (tid == 0) atomicOr(&wk.segs[t.seg].flags, kSegFault);
+      mbar_wait(&stage_bar, stage_phase ^ 1u, kStageWaitNs);
+      return;
+    }
     const SmemBytes sd{sdata, boff};
 
     // -- links of the new positions [lstart, nreg): the previous position
@@ -439,9 +502,17 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
           idle = __ballot_sync(kAll, i == kAll);
         }
         if (idle == kAll) break;
-        if (i != kAll && lz_step(st, sd, link, cfg.nice, cfg.miss)) {
-          F[i] = st.best >= 3 ? (st.best << 16) | st.bd : 0u;
-          i = kAll;
+        // a few chain steps per round: the warp re-balances (ballot, new
+        // positions for lanes whose chain ended) once per kStepsPerRound steps
+        if (i != kAll) {
+#pragma unroll 1
+          for (int k = 0; k < kStepsPerRound; ++k) {
+            if (lz_step(st, sd, link, cfg.nice, cfg.miss)) {
+              F[i] = st.best >= 3 ? (st.best << 16) | st.bd : 0u;
+              i = kAll;
+              break;
+            }
+          }
         }
       }
     }
@@ -625,6 +696,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     }
     prev_rs = rs;
     prev_nreg = nreg;
+    fence_proxy_async_smem();  // this tile's reads and writes of the staged bytes, before the next copy
     __syncthreads();
   }
 }
