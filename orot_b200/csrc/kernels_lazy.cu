@@ -101,12 +101,15 @@ __device__ __forceinline__ uint32_t hash15(uint32_t v) { return (v * 0x9E3779B1u
 struct LzState {
   uint32_t r, v4p, h16p, q, maxm, best, bd;
   uint32_t pqr;  // the 4 bytes of r ending at byte `best` (the quick reject's p side), once best >= 4
+  uint32_t nl;   // link of the current candidate (loaded with it, so the next step does not wait for it)
   int steps, miss, bud;
 };
 
-__device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, uint32_t r, uint32_t maxm, int chain) {
+__device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t r,
+                                         uint32_t maxm, int chain) {
   s.r = r;
   s.q = r;
+  s.nl = link[r];
   s.v4p = sd.load4(r);
   s.h16p = hash16(s.v4p);
   s.maxm = maxm;
@@ -122,11 +125,12 @@ __device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, uint32
 __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const uint16_t* __restrict__ link, int nice,
                                         int miss_limit) {
   if (s.bud-- <= 0) return true;
-  const uint32_t l = link[s.q];
+  const uint32_t l = s.nl;
   if (!l) return true;
   s.q -= l;
   const uint32_t q = s.q, r = s.r;
   if (r - q > 32767u) return true;
+  s.nl = link[q];
   const uint32_t v = sd.load4(q);
   if (v != s.v4p && hash16(v) != s.h16p) return false;  // same 15-bit bucket, other 16-bit chain
   if (s.steps-- == 0) return true;
@@ -136,11 +140,22 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
   // byte `best`: a longer match needs all of them
   const uint32_t maxm = s.maxm, mb = s.best;
   if (mb >= 4 && mb < maxm && sd.load4(q + mb - 3) != s.pqr) return false;
+  // the comparison from byte 4: aligned words on both sides, each loaded once
   uint32_t len = 4;
-  while (len < maxm) {
-    const uint32_t x = sd.load4(r + len) ^ sd.load4(q + len);
-    if (x) { len += (__ffs(x) - 1) >> 3; break; }
-    len += 4;
+  {
+    const uint32_t pi = r + 4 + sd.boff, qi = q + 4 + sd.boff;
+    const uint32_t ps = (pi & 3) * 8, qs = (qi & 3) * 8;
+    const uint32_t* pw = sd.w + (pi >> 2);
+    const uint32_t* qw = sd.w + (qi >> 2);
+    uint32_t plo = pw[0], qlo = qw[0];
+    for (uint32_t k = 1; len < maxm; ++k) {
+      const uint32_t phi = pw[k], qhi = qw[k];
+      const uint32_t x = __funnelshift_r(plo, phi, ps) ^ __funnelshift_r(qlo, qhi, qs);
+      if (x) { len += (__ffs(x) - 1) >> 3; break; }
+      len += 4;
+      plo = phi;
+      qlo = qhi;
+    }
   }
   if (len > maxm) len = maxm;
   if (len > s.best) {
@@ -495,7 +510,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
           const uint32_t take = min(uint32_t(__popc(idle)), avail);
           if (i == kAll && __popc(idle & lt) < take) {
             i = pool + __popc(idle & lt);
-            lz_begin(st, sd, ts - rs + i, min(258u, tl - i), cfg.chain);
+            lz_begin(st, sd, link, ts - rs + i, min(258u, tl - i), cfg.chain);
           }
           pool += take;
           avail -= take;
