@@ -64,7 +64,7 @@ static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words 
 static_assert((kRegion + 31) / 32 * 8 <= kFBytes, "first/last marks of every link chunk fit F");
 
 constexpr uint32_t kSerialParse = 128;  // at most this many match positions: serial parse
-constexpr int kStepsPerRound = 4;       // chain steps a searching lane takes between re-balancing rounds
+constexpr int kStepsPerRound = 8;       // chain steps a searching lane takes between re-balancing rounds
 
 // chain, nice, lazy depth, miss limit, optimal parse (levels 10-12)
 struct LazyCfg { int chain, nice, lazy, miss, opt; };
