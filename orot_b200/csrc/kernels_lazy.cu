@@ -75,7 +75,6 @@ constexpr int kStepsPerRound = 8;       // chain steps a searching lane takes be
 constexpr int kChain0 = 8;
 constexpr int kMaxRefine = 4;
 constexpr uint32_t kDenseDist = 64;
-constexpr uint32_t kWarpSearchMax = 96;  // refinement searches per round done by whole warps, at most
 
 // chain, nice, lazy depth, miss limit, optimal parse (levels 10-12)
 struct LazyCfg { int chain, nice, lazy, miss, opt; };
@@ -808,26 +807,20 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
           }
         }
         __syncthreads();
-        if (tid == 0) scan[60] = 0;
-        __syncthreads();
-        uint32_t todo_n = 0;
+        uint32_t todo_any = 0;
         for (uint32_t w = tid; w < kFmWords; w += blockDim.x) {
           const uint32_t todo = needm[w] & ~fullm[w];
           needm[w] = todo;
           fullm[w] |= todo;
-          todo_n += __popc(todo);
+          todo_any |= todo;
         }
-        if (todo_n) atomicAdd(&scan[60], todo_n);
-        __syncthreads();
-        const uint32_t ntodo = scan[60];
-        if (!ntodo) break;
+        if (!__syncthreads_or(todo_any != 0)) break;
         for (uint32_t w = tid; w < kFmWords; w += blockDim.x) hd[w] = 0;  // heads of the next parse
         if (tid == 0) scan[62] = 0;
         __syncthreads();
-        // Few positions, each a long walk: a warp per position (its time is the
-        // walk's length / 32); many: a lane per position (its time is the
-        // longest walk).  Both give the same matches (a test knob forces lanes).
-        if ((sg.flags & kSegLaneSearch) || ntodo > kWarpSearchMax)
+        // few positions, each a long walk: a warp per position (one lane per
+        // position with the test knob that checks the two agree)
+        if (sg.flags & kSegLaneSearch)
           search_positions(sd, link, F, needm, nsearch, ts - rs, tl, cfg.chain, cfg.nice, cfg.miss, &scan[62], nullptr);
         else
           search_positions_warp(sd, link, F, needm, nsearch, ts - rs, tl, cfg.chain, cfg.nice, cfg.miss, &scan[62]);
