@@ -152,9 +152,6 @@ Engine::Engine() {
     const long t = std::strtol(v, nullptr, 10);
     if (t >= 32 && t <= 65536 && t % 32 == 0) tile_override = uint32_t(t);
   }
-  // Dense-tile refinement searched by one lane per position instead of a warp
-  // (tests compare the two, which must agree).
-  if (const char* v = std::getenv("OROT_B200_LANE_REFINE")) lane_refine = v[0] == '1';
   // Lazy-level run length override (tiles per CTA, 1..kLazyRun) for tests.
   if (const char* v = std::getenv("OROT_B200_LAZY_RUN")) {
     const long r = std::strtol(v, nullptr, 10);
@@ -235,8 +232,7 @@ bool Engine::plan(const std::vector<Job>& jobs) {
       g.len = uint32_t(len);
       g.stream = uint32_t(ji);
       g.level = lv;
-      g.flags = (k + 1 == nseg && !(j.mode & kStreamOpen) ? kSegLast : 0) | (j.parallel ? 0 : kSegWholeBuf) |
-                (lane_refine ? kSegLaneSearch : 0);
+      g.flags = (k + 1 == nseg && !(j.mode & kStreamOpen) ? kSegLast : 0) | (j.parallel ? 0 : kSegWholeBuf);
       g.tile_first = uint32_t(tiles.size());
       const int hb = lv <= 0 ? 0 : lv == 1 ? 12 : lv <= 3 ? 14 : 0;
       const uint32_t H = hb ? (1u << hb) : 0;

@@ -24,7 +24,6 @@ constexpr int kBlkStored = 0, kBlkFixed = 1, kBlkDynamic = 2;
 constexpr uint32_t kSegLast = 1u;        // BFINAL block of its stream
 constexpr uint32_t kSegWholeBuf = 2u;    // whole-buffer rule: all-literal parse -> stored
 constexpr uint32_t kSegFault = 8u;       // set by a kernel that could not finish the segment (its stream fails)
-constexpr uint32_t kSegLaneSearch = 16u; // levels 4-9, tests: refine dense tiles with one lane per position
 
 // Stream error codes written to Stream::error.
 constexpr uint32_t kErrNone = 0, kErrCapacity = 1, kErrInternal = 2;

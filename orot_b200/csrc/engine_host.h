@@ -92,7 +92,6 @@ class Engine {
   cudaGraphExec_t graph_exec = nullptr;
   uint32_t tile_override = 0;
   uint32_t lazy_run_override = 0;
-  bool lane_refine = false;  // tests: dense-tile refinement with one lane per position
 
   // planned tables (host copies)
   std::vector<Stream> streams;

@@ -113,7 +113,6 @@ struct LzState {
   uint32_t pqr;  // the 4 bytes of r ending at byte `best` (the quick reject's p side), once best >= 4
   uint32_t nl;   // link of the current candidate (loaded with it, so the next step does not wait for it)
   int steps, miss, bud;
-  bool cut;      // the walk ended at its step or candidate budget (a longer chain might find more)
 };
 
 __device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t r,
@@ -130,13 +129,12 @@ __device__ __forceinline__ void lz_begin(LzState& s, const SmemBytes& sd, const 
   s.steps = chain;
   s.miss = 0;
   s.bud = 2 * chain + 64;  // bounds the filtered candidates too
-  s.cut = false;
 }
 
 // One candidate; returns true once the search has ended.
 __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const uint16_t* __restrict__ link, int nice,
                                         int miss_limit) {
-  if (s.bud-- <= 0) return s.cut = true;
+  if (s.bud-- <= 0) return true;
   const uint32_t l = s.nl;
   if (!l) return true;
   s.q -= l;
@@ -145,7 +143,7 @@ __device__ __forceinline__ bool lz_step(LzState& s, const SmemBytes& sd, const u
   s.nl = link[q];
   const uint32_t v = sd.load4(q);
   if (v != s.v4p && hash16(v) != s.h16p) return false;  // same 15-bit bucket, other 16-bit chain
-  if (s.steps-- == 0) return s.cut = true;
+  if (s.steps-- == 0) return true;
   if (v != s.v4p) return ++s.miss >= miss_limit;
   s.miss = 0;
   // quick reject (src/deflate/lz77.cpp:137-142), on the 4 bytes ending at
@@ -321,17 +319,14 @@ __device__ __forceinline__ void clear_bits_atomic(uint32_t* bm, uint32_t lo, uin
 
 // Searches the tile positions below nsearch whose bit is set in todo (every
 // position when todo is null) with chains of `chain` steps and writes their
-// matches into F.  With `done` set, a position whose walk ended before its
-// step or candidate budget (chain end, window edge, miss limit, nice length)
-// gets its bit set there: a longer chain would find the same match.  Warps
-// take 32-position chunks from *counter (zero on entry); a lane whose chain
-// has ended takes the next position of its warp's chunk at once, so lanes
-// stay busy across chains of very different lengths, and the warp
-// re-balances once per kStepsPerRound chain steps.  Every thread of the CTA
-// calls it.
+// matches into F.  Warps take 32-position chunks from *counter (zero on
+// entry); a lane whose chain has ended takes the next position of its warp's
+// chunk at once, so lanes stay busy across chains of very different lengths,
+// and the warp re-balances once per kStepsPerRound chain steps.  Every thread
+// of the CTA calls it.
 __device__ __noinline__ void search_positions(const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t* F,
                                               const uint32_t* todo, uint32_t nsearch, uint32_t off, uint32_t tl,
-                                              int chain, int nice, int miss, uint32_t* counter, uint32_t* done) {
+                                              int chain, int nice, int miss, uint32_t* counter) {
   const uint32_t lane = threadIdx.x & 31;
   const uint32_t nch = (nsearch + 31) / 32;
   const uint32_t lt = (1u << lane) - 1;
@@ -371,121 +366,10 @@ __device__ __noinline__ void search_positions(const SmemBytes& sd, const uint16_
       for (int k = 0; k < kStepsPerRound; ++k) {
         if (lz_step(st, sd, link, nice, miss)) {
           F[i] = st.best >= 3 ? (st.best << 16) | st.bd : 0u;
-          if (done && !st.cut) atomicOr(&done[i >> 5], 1u << (i & 31));
           i = kAll;
           break;
         }
       }
-    }
-  }
-}
-
-// The full chain search of position r by a whole warp, with exactly the
-// result of lz_begin + lz_step (same candidates in the same order, the same
-// step, miss, budget, window and nice rules): the chain is followed 32
-// candidates at a time (every lane walks the links, lane k keeps candidate
-// k), the 32 candidates are compared at once, and the batch's end point
-// (budget, chain end, window edge, step limit, miss limit, nice length) is
-// found from ballots.  Used where few positions need a long search each.
-// Every lane of the warp calls it; returns the match (len << 16 | dist) or 0.
-__device__ uint32_t search_warp(const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t r, uint32_t maxm,
-                                int chain, int nice, int miss_limit) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t v4p = sd.load4(r), h16p = hash16(v4p);
-  uint32_t best = 2, bd = 0, q = r, nl = link[r];
-  int steps = chain, miss = 0, bud = 2 * chain + 64;
-  for (;;) {
-    // gather up to 32 candidates in chain order
-    uint32_t myq = 0, n = 0;
-    bool walk_end = false;
-    for (uint32_t k = 0; k < 32; ++k) {
-      if (bud-- <= 0 || nl == 0) { walk_end = true; break; }
-      q -= nl;
-      if (r - q > 32767u) { walk_end = true; break; }
-      if (lane == k) myq = q;
-      nl = link[q];
-      ++n;
-    }
-    const bool have = lane < n;
-    uint32_t v = have ? sd.load4(myq) : 0u;
-    const bool counted = have && (v == v4p || hash16(v) == h16p);
-    const bool hit = counted && v == v4p;
-    const uint32_t cm = __ballot_sync(kAll, counted), hm = __ballot_sync(kAll, hit);
-    // step and miss limits over the counted candidates, in order
-    uint32_t e_stop = n;     // first candidate not examined (step limit) or n
-    uint32_t e_miss = 32;    // candidate at which the miss limit is reached
-    {
-      uint32_t c = cm;
-      while (c) {
-        const uint32_t k = __ffs(c) - 1;
-        c &= c - 1;
-        if (steps-- == 0) { e_stop = k; steps = 0; break; }
-        if ((hm >> k) & 1u) {
-          miss = 0;
-        } else if (++miss >= miss_limit) {
-          e_miss = k;
-          break;
-        }
-      }
-    }
-    const uint32_t e_pre = min(e_stop, e_miss);
-    // lengths of the hits before the step / miss end
-    uint32_t len = 0;
-    if (hit && lane < e_pre) {
-      len = 4;
-      const uint32_t pi = r + 4 + sd.boff, qi = myq + 4 + sd.boff;
-      const uint32_t ps = (pi & 3) * 8, qs = (qi & 3) * 8;
-      const uint32_t* pw = sd.w + (pi >> 2);
-      const uint32_t* qw = sd.w + (qi >> 2);
-      uint32_t plo = pw[0], qlo = qw[0];
-      for (uint32_t k = 1; len < maxm; ++k) {
-        const uint32_t phi = pw[k], qhi = qw[k];
-        const uint32_t x = __funnelshift_r(plo, phi, ps) ^ __funnelshift_r(qlo, qhi, qs);
-        if (x) { len += (__ffs(x) - 1) >> 3; break; }
-        len += 4;
-        plo = phi;
-        qlo = qhi;
-      }
-      if (len > maxm) len = maxm;
-    }
-    // the first candidate longer than the best so far that reaches nice
-    // (or the longest possible) ends the walk there
-    const uint32_t nm = __ballot_sync(kAll, len > best && (int(len) >= nice || len >= maxm));
-    const uint32_t e_nice = nm ? __ffs(nm) - 1 : 32u;
-    const uint32_t e = min(e_pre, e_nice);
-    const bool eligible = len > 0 && (lane < e || lane == e_nice) && lane <= e;
-    // longest; ties keep the nearest (the lowest lane)
-    const uint32_t key = eligible ? (len << 8) | (31 - lane) : 0u;
-    const uint32_t top = __reduce_max_sync(kAll, key);
-    if (top && (top >> 8) > best) {
-      const uint32_t kbest = 31 - (top & 0xFFu);
-      best = top >> 8;
-      bd = r - __shfl_sync(kAll, myq, kbest);
-    }
-    if (e < n || walk_end || e_nice < 32) break;
-  }
-  return best >= 3 ? (best << 16) | bd : 0u;
-}
-
-// Warps take 32-position chunks of `todo` from *counter (zero on entry) and
-// search each position of a chunk with search_warp.  Every thread calls it.
-__device__ __noinline__ void search_positions_warp(const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t* F,
-                                                   const uint32_t* todo, uint32_t nsearch, uint32_t off, uint32_t tl,
-                                                   int chain, int nice, int miss, uint32_t* counter) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t nch = (nsearch + 31) / 32;
-  for (;;) {
-    uint32_t c = 0;
-    if (lane == 0) c = atomicAdd(counter, 1u);
-    c = __shfl_sync(kAll, c, 0);
-    if (c >= nch) break;
-    const uint32_t valid = nsearch - c * 32 >= 32 ? kAll : ((1u << (nsearch - c * 32)) - 1u);
-    uint32_t rem = todo[c] & valid;
-    while (rem) {
-      const uint32_t i = c * 32 + __ffs(rem) - 1;
-      rem &= rem - 1;
-      const uint32_t f = search_warp(sd, link, off + i, min(258u, tl - i), chain, nice, miss);
-      if (lane == 0) F[i] = f;
     }
   }
 }
@@ -724,9 +608,8 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
       for (uint32_t w = tid; w < kFmWords; w += blockDim.x) fullm[w] = refine ? 0u : kAll;
       if (tid == 0) scan[62] = 0;
       __syncthreads();
-      // (a short walk that ended before its budget is already the full walk's result)
       search_positions(sd, link, F, nullptr, nsearch, ts - rs, tl, refine ? kChain0 : cfg.chain, cfg.nice, cfg.miss,
-                       &scan[62], refine ? fullm : nullptr);
+                       &scan[62]);
       __syncthreads();
       for (int round = 0;; ++round) {
         for (uint32_t c = wid; c < kFmWords; c += blockDim.x >> 5) {
@@ -818,12 +701,7 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
         for (uint32_t w = tid; w < kFmWords; w += blockDim.x) hd[w] = 0;  // heads of the next parse
         if (tid == 0) scan[62] = 0;
         __syncthreads();
-        // few positions, each a long walk: a warp per position (one lane per
-        // position with the test knob that checks the two agree)
-        if (sg.flags & kSegLaneSearch)
-          search_positions(sd, link, F, needm, nsearch, ts - rs, tl, cfg.chain, cfg.nice, cfg.miss, &scan[62], nullptr);
-        else
-          search_positions_warp(sd, link, F, needm, nsearch, ts - rs, tl, cfg.chain, cfg.nice, cfg.miss, &scan[62]);
+        search_positions(sd, link, F, needm, nsearch, ts - rs, tl, cfg.chain, cfg.nice, cfg.miss, &scan[62]);
         __syncthreads();
       }
       for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;

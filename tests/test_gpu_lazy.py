@@ -114,25 +114,3 @@ def test_lazy_window_runs_match_single_tiles(gpu, oracle, level, monkeypatch):
         assert zlib.decompress(out) == d
     ref = oracle.compress(bufs[1], level, 1)
     assert within(len(outs["16"][1]), len(ref)), (len(outs["16"][1]), len(ref))
-
-
-@pytest.mark.parametrize("level", [4, 6, 9])
-def test_warp_search_equals_lane_search(gpu, level, monkeypatch):
-    """Dense tiles (short repeat distances) are refined with a warp per
-    searched position; the warp search follows the same chain rules as one
-    lane per position (OROT_B200_LANE_REFINE=1), so the bytes are identical."""
-    sizes = [3 << 20, 1 << 20, 300001]
-    kinds = [synth.PERIODIC, synth.MIXED, synth.ZEROS]
-    bufs = [synth.gen(n, k, 90 + i) for i, (n, k) in enumerate(zip(sizes, kinds))]
-    outs = {}
-    for lane in ("0", "1"):
-        monkeypatch.setenv("OROT_B200_LANE_REFINE", lane)
-        b = gpu.DeviceBatch()
-        b.load(b"".join(bufs), sizes, level, gpu.Format.Raw)
-        b.run()
-        got = b.sizes()
-        outs[lane] = [b.output(i, got[i]) for i in range(len(sizes))]
-        b.close()
-    for d, o in zip(bufs, outs["0"]):
-        assert zlib.decompress(o, -15) == d
-    assert outs["0"] == outs["1"]
