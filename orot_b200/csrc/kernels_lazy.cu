@@ -57,7 +57,7 @@ constexpr uint32_t kTokBytes = T * 4;
 constexpr uint32_t kFmWords = T / 32;
 constexpr uint32_t kOptBytes = T * 2 + 320 * 2 + 260 * 2;      // optimal parse: choice[T], symbol and length costs
 constexpr uint32_t kSmemLz = kDataBytes + kLinkBytes + kTblBytes + kFBytes + kTokBytes + kFmWords * 4 + 320 * 4 +
-                             64 * 4 + kOptBytes + 2 * kFmWords * 4;
+                             64 * 4 + kOptBytes;
 static_assert(T % 32 == 0, "tiles are whole windows of 32 positions");
 static_assert(kSmemLz <= 227 * 1024, "one CTA per SM");
 static_assert((T & 1) == 0 && (W & 1) == 0, "window shifts move whole u32 words of links");
@@ -65,16 +65,6 @@ static_assert((kRegion + 31) / 32 * 8 <= kFBytes, "first/last marks of every lin
 
 constexpr uint32_t kSerialParse = 128;  // at most this many match positions: serial parse
 constexpr int kStepsPerRound = 8;       // chain steps a searching lane takes between re-balancing rounds
-// Dense tiles (most positions repeat a context at most kDenseDist bytes back:
-// short periods, fills) at levels 4-9 are searched with chains of at most
-// kChain0 steps first, then with the level's full chain only at the positions
-// the lazy parse reads (every position but the inside of a chosen match), and
-// parsed again, at most kMaxRefine times; once a parse reads only fully
-// searched positions it is the parse of a full search everywhere.  Most of a
-// dense tile lies inside long matches, so most full searches are skipped.
-constexpr int kChain0 = 8;
-constexpr int kMaxRefine = 4;
-constexpr uint32_t kDenseDist = 64;
 
 // chain, nice, lazy depth, miss limit, optimal parse (levels 10-12)
 struct LazyCfg { int chain, nice, lazy, miss, opt; };
@@ -291,89 +281,6 @@ __device__ __forceinline__ uint16_t sym_cost(uint32_t count, uint32_t total) {
   return uint16_t(16.0f * fminf(fmaxf(b, 1.0f), 15.0f) + 0.5f);
 }
 
-// Position of the n-th (from 0) set bit of m; m has more than n set bits.
-__device__ __forceinline__ uint32_t select_bit(uint32_t m, uint32_t n) {
-  uint32_t base = 0;
-#pragma unroll
-  for (uint32_t s = 16; s > 0; s >>= 1) {
-    const uint32_t lo = __popc(m & ((1u << s) - 1u));
-    if (n >= lo) {
-      n -= lo;
-      m >>= s;
-      base += s;
-    }
-  }
-  return base;
-}
-
-// Clears the bits of positions [lo, hi) where other threads clear other
-// ranges that may share a word.
-__device__ __forceinline__ void clear_bits_atomic(uint32_t* bm, uint32_t lo, uint32_t hi) {
-  while (lo < hi) {
-    const uint32_t w = lo >> 5, b0 = lo & 31, n = min(32u - b0, hi - lo);
-    const uint32_t mask = (n == 32 ? kAll : ((1u << n) - 1)) << b0;
-    atomicAnd(&bm[w], ~mask);
-    lo += n;
-  }
-}
-
-// Searches the tile positions below nsearch whose bit is set in todo (every
-// position when todo is null) with chains of `chain` steps and writes their
-// matches into F.  Warps take 32-position chunks from *counter (zero on
-// entry); a lane whose chain has ended takes the next position of its warp's
-// chunk at once, so lanes stay busy across chains of very different lengths,
-// and the warp re-balances once per kStepsPerRound chain steps.  Every thread
-// of the CTA calls it.
-__device__ __noinline__ void search_positions(const SmemBytes& sd, const uint16_t* __restrict__ link, uint32_t* F,
-                                              const uint32_t* todo, uint32_t nsearch, uint32_t off, uint32_t tl,
-                                              int chain, int nice, int miss, uint32_t* counter) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t nch = (nsearch + 31) / 32;
-  const uint32_t lt = (1u << lane) - 1;
-  uint32_t rem = 0, cbase = 0;  // warp-uniform: positions of the chunk not yet taken
-  bool more = true;
-  uint32_t i = kAll;            // this lane's position
-  LzState st;
-  for (;;) {
-    uint32_t idle = __ballot_sync(kAll, i == kAll);
-    while (idle && (rem || more)) {
-      if (!rem) {
-        uint32_t c = 0;
-        if (lane == 0) c = atomicAdd(counter, 1u);
-        c = __shfl_sync(kAll, c, 0);
-        if (c >= nch) {
-          more = false;
-          break;
-        }
-        cbase = c * 32;
-        const uint32_t valid = nsearch - cbase >= 32 ? kAll : ((1u << (nsearch - cbase)) - 1u);
-        rem = (todo ? todo[c] : kAll) & valid;
-        continue;
-      }
-      const uint32_t take = min(uint32_t(__popc(idle)), uint32_t(__popc(rem)));
-      const uint32_t rank = __popc(idle & lt);
-      if (i == kAll && rank < take) {
-        i = cbase + select_bit(rem, rank);
-        lz_begin(st, sd, link, off + i, min(258u, tl - i), chain);
-      }
-      const uint32_t lastbit = select_bit(rem, take - 1);
-      rem &= lastbit >= 31 ? 0u : (kAll << (lastbit + 1));
-      idle = __ballot_sync(kAll, i == kAll);
-    }
-    if (idle == kAll) break;
-    if (i != kAll) {
-#pragma unroll 1
-      for (int k = 0; k < kStepsPerRound; ++k) {
-        if (lz_step(st, sd, link, nice, miss)) {
-          F[i] = st.best >= 3 ? (st.best << 16) | st.bd : 0u;
-          i = kAll;
-          break;
-        }
-      }
-    }
-  }
-}
-
 // -- staging by the bulk-copy engine (TMA, untiled; the source is this GPU's
 // own input arena, no multicast): one thread starts the copy of a tile's
 // window into shared memory and the CTA waits on an mbarrier for its bytes.
@@ -439,8 +346,6 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
   uint16_t* choice = reinterpret_cast<uint16_t*>(scan + 64);  // optimal parse: token length at each position
   uint16_t* scost = choice + T;                              // symbol costs, 1/16 bit: 0-255 literals, 257+ lengths, 288+ distances
   uint16_t* lcost = scost + 320;                             // cost of a match length 0..258 (code + extra bits)
-  uint32_t* fullm = reinterpret_cast<uint32_t*>(lcost + 260);  // dense tiles: a bit per position searched fully
-  uint32_t* needm = fullm + kFmWords;                          // positions the parse reads, then those still to search
   const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
   if (blockIdx.x >= nruns) return;
@@ -576,9 +481,64 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
     if (tid == 0) scan[62] = 0;
     __syncthreads();
 
-    // -- searches.  Every position of a tile is searched with the level's
-    // full chain, except in dense tiles (see kChain0): there a short-chain
-    // search everywhere is refined where the lazy parse reads.
+    // -- searches at every tile position.  Warps take 32-position chunks; a
+    // lane whose chain has ended takes the next position of its warp's chunk
+    // at once, so lanes stay busy across chains of very different lengths.
+    {
+      const uint32_t nsearch = tl >= 4 ? tl - 3 : 0;
+      const uint32_t nch = (nsearch + 31) / 32;
+      for (uint32_t i = nsearch + tid; i < kFmWords * 32; i += blockDim.x) F[i] = 0;
+      const uint32_t lt = (1u << lane) - 1;
+      uint32_t pool = 0, avail = 0;  // warp-uniform: next position of the chunk, positions left
+      bool more = true;
+      uint32_t i = kAll;             // this lane's position
+      LzState st;
+      for (;;) {
+        uint32_t idle = __ballot_sync(kAll, i == kAll);
+        while (idle && (avail || more)) {
+          if (!avail) {
+            uint32_t c = 0;
+            if (lane == 0) c = atomicAdd(&scan[62], 1u);
+            c = __shfl_sync(kAll, c, 0);
+            if (c >= nch) {
+              more = false;
+              break;
+            }
+            pool = c * 32;
+            avail = min(32u, nsearch - pool);
+          }
+          const uint32_t take = min(uint32_t(__popc(idle)), avail);
+          if (i == kAll && __popc(idle & lt) < take) {
+            i = pool + __popc(idle & lt);
+            lz_begin(st, sd, link, ts - rs + i, min(258u, tl - i), cfg.chain);
+          }
+          pool += take;
+          avail -= take;
+          idle = __ballot_sync(kAll, i == kAll);
+        }
+        if (idle == kAll) break;
+        // a few chain steps per round: the warp re-balances (ballot, new
+        // positions for lanes whose chain ended) once per kStepsPerRound steps
+        if (i != kAll) {
+#pragma unroll 1
+          for (int k = 0; k < kStepsPerRound; ++k) {
+            if (lz_step(st, sd, link, cfg.nice, cfg.miss)) {
+              F[i] = st.best >= 3 ? (st.best << 16) | st.bd : 0u;
+              i = kAll;
+              break;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (uint32_t c = wid; c < kFmWords; c += blockDim.x >> 5) {
+      const uint32_t b = __ballot_sync(kAll, F[c * 32 + lane] != 0);
+      if (lane == 0) fm[c] = b;
+    }
+    for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
+    __syncthreads();
+
     // -- parse (reference lazy rule, lz77.cpp:449-493, with n = tile end).
     // A parse step depends only on its start position (the head), so the
     // heads are found in parallel: (1) each lane of warp 0 parses one 1/32 of
@@ -589,122 +549,62 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
       uint32_t* hd = hist;  // heads, a bit per position (hist is zero until the histogram)
       uint32_t* sx = scan;  // where each segment's parse leaves it
       const uint32_t S = (tl + 31) / 32;
-      const uint32_t nsearch = tl >= 4 ? tl - 3 : 0;
-      for (uint32_t i = nsearch + tid; i < kFmWords * 32; i += blockDim.x) F[i] = 0;
-      if (tid == 0) scan[61] = 0;
-      __syncthreads();
-      bool refine = false;
-      if (!cfg.opt && cfg.chain > kChain0) {
-        uint32_t near = 0;
-        for (uint32_t i = tid; i < tl; i += blockDim.x) {
-          const uint32_t l = link[ts - rs + i];
-          near += (l != 0 && l <= kDenseDist) ? 1u : 0u;
-        }
-        near = __reduce_add_sync(kAll, near);
-        if (lane == 0 && near) atomicAdd(&scan[61], near);
-        __syncthreads();
-        refine = uint64_t(scan[61]) * 10 >= uint64_t(tl) * 9;  // block-uniform
+      uint32_t nf = 0;  // positions with a match: few -> one lane parses alone
+      if (wid == 0) {
+        for (uint32_t w = lane; w < kFmWords; w += 32) nf += __popc(fm[w]);
+        nf = __reduce_add_sync(kAll, nf);
       }
-      for (uint32_t w = tid; w < kFmWords; w += blockDim.x) fullm[w] = refine ? 0u : kAll;
-      if (tid == 0) scan[62] = 0;
-      __syncthreads();
-      search_positions(sd, link, F, nullptr, nsearch, ts - rs, tl, refine ? kChain0 : cfg.chain, cfg.nice, cfg.miss,
-                       &scan[62]);
-      __syncthreads();
-      for (int round = 0;; ++round) {
-        for (uint32_t c = wid; c < kFmWords; c += blockDim.x >> 5) {
-          const uint32_t fb = __ballot_sync(kAll, F[c * 32 + lane] != 0);
-          if (lane == 0) fm[c] = fb;
-        }
-        __syncthreads();
-        uint32_t nf = 0;  // positions with a match: few -> one lane parses alone
-        if (wid == 0) {
-          for (uint32_t w = lane; w < kFmWords; w += 32) nf += __popc(fm[w]);
-          nf = __reduce_add_sync(kAll, nf);
-        }
-        if (wid == 0 && nf <= kSerialParse) {
-          if (lane == 0) {
-            uint32_t i = 0;
-            while ((i = next_head(fm, i, tl)) < tl) {
-              hd[i >> 5] |= 1u << (i & 31);
-              const uint2 m = lazy_step(F, i, tl, cfg.lazy);
-              i = (m.x & 0xFFFFu) + (m.y >> 16);
-            }
-          }
-        } else if (wid == 0) {
-          const uint32_t a = min(lane * S, tl), b = min(a + S, tl);
-          uint32_t i = a;
-          while (i < b) {
-            i = next_head(fm, i, tl);
-            if (i >= b) break;
-            atomicOr(&hd[i >> 5], 1u << (i & 31));
+      if (wid == 0 && nf <= kSerialParse) {
+        if (lane == 0) {
+          uint32_t i = 0;
+          while ((i = next_head(fm, i, tl)) < tl) {
+            hd[i >> 5] |= 1u << (i & 31);
             const uint2 m = lazy_step(F, i, tl, cfg.lazy);
             i = (m.x & 0xFFFFu) + (m.y >> 16);
           }
-          sx[lane] = i;
-          __syncwarp();
-          if (lane == 0) {
-            uint32_t e = sx[0];
-            for (uint32_t sgi = 1; sgi < 32; ++sgi) {
-              const uint32_t a2 = min(sgi * S, tl), b2 = min(a2 + S, tl);
-              if (a2 >= b2) break;
-              clear_bits(hd, a2, min(e, b2));
-              if (e >= b2) continue;
-              uint32_t i2 = e;
-              for (;;) {
-                const uint32_t h = next_head(fm, i2, tl);
-                if (h >= b2) {
-                  e = h;
-                  break;
-                }
-                if ((hd[h >> 5] >> (h & 31)) & 1u) {
-                  e = sx[sgi];
-                  break;
-                }
-                hd[h >> 5] |= 1u << (h & 31);
-                const uint2 m = lazy_step(F, h, tl, cfg.lazy);
-                i2 = (m.x & 0xFFFFu) + (m.y >> 16);
-                clear_bits(hd, h + 1, min(i2, b2));
-                if (i2 >= b2) {
-                  e = i2;
-                  break;
-                }
+        }
+      } else if (wid == 0) {
+        const uint32_t a = min(lane * S, tl), b = min(a + S, tl);
+        uint32_t i = a;
+        while (i < b) {
+          i = next_head(fm, i, tl);
+          if (i >= b) break;
+          atomicOr(&hd[i >> 5], 1u << (i & 31));
+          const uint2 m = lazy_step(F, i, tl, cfg.lazy);
+          i = (m.x & 0xFFFFu) + (m.y >> 16);
+        }
+        sx[lane] = i;
+        __syncwarp();
+        if (lane == 0) {
+          uint32_t e = sx[0];
+          for (uint32_t sgi = 1; sgi < 32; ++sgi) {
+            const uint32_t a2 = min(sgi * S, tl), b2 = min(a2 + S, tl);
+            if (a2 >= b2) break;
+            clear_bits(hd, a2, min(e, b2));
+            if (e >= b2) continue;
+            uint32_t i2 = e;
+            for (;;) {
+              const uint32_t h = next_head(fm, i2, tl);
+              if (h >= b2) {
+                e = h;
+                break;
+              }
+              if ((hd[h >> 5] >> (h & 31)) & 1u) {
+                e = sx[sgi];
+                break;
+              }
+              hd[h >> 5] |= 1u << (h & 31);
+              const uint2 m = lazy_step(F, h, tl, cfg.lazy);
+              i2 = (m.x & 0xFFFFu) + (m.y >> 16);
+              clear_bits(hd, h + 1, min(i2, b2));
+              if (i2 >= b2) {
+                e = i2;
+                break;
               }
             }
           }
         }
-        __syncthreads();
-        if (!refine || round == kMaxRefine) break;
-        // positions the parse read: every position but the inside of a match
-        // (a head's lazy steps read at most one position past the match start)
-        for (uint32_t w = tid; w < kFmWords; w += blockDim.x) {
-          const uint32_t b0 = w * 32;
-          needm[w] = b0 >= tl ? 0u : (tl - b0 >= 32 ? kAll : ((1u << (tl - b0)) - 1u));
-        }
-        __syncthreads();
-        for (uint32_t i = tid; i < tl; i += blockDim.x) {
-          if ((hd[i >> 5] >> (i & 31)) & 1u) {
-            const uint2 m = lazy_step(F, i, tl, cfg.lazy);
-            const uint32_t at = m.x & 0xFFFFu;
-            clear_bits_atomic(needm, at + 2, at + (m.y >> 16));
-          }
-        }
-        __syncthreads();
-        uint32_t todo_any = 0;
-        for (uint32_t w = tid; w < kFmWords; w += blockDim.x) {
-          const uint32_t todo = needm[w] & ~fullm[w];
-          needm[w] = todo;
-          fullm[w] |= todo;
-          todo_any |= todo;
-        }
-        if (!__syncthreads_or(todo_any != 0)) break;
-        for (uint32_t w = tid; w < kFmWords; w += blockDim.x) hd[w] = 0;  // heads of the next parse
-        if (tid == 0) scan[62] = 0;
-        __syncthreads();
-        search_positions(sd, link, F, needm, nsearch, ts - rs, tl, cfg.chain, cfg.nice, cfg.miss, &scan[62]);
-        __syncthreads();
       }
-      for (uint32_t i = tid; i < T; i += blockDim.x) tok_s[i] = 0;
       __syncthreads();
       for (uint32_t i = tid; i < tl; i += blockDim.x) {
         if ((hd[i >> 5] >> (i & 31)) & 1u) {
