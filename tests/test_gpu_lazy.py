@@ -95,8 +95,9 @@ def test_lazy_window_runs_match_single_tiles(gpu, oracle, level, monkeypatch):
     """A CTA that slides its window over a run of tiles emits exactly the
     tokens of one CTA per tile (run length forced to 1), and both stay within
     the size bound of the reference."""
-    sizes = [40 << 20, 5 << 20, 4128 * 16 + 1, 4128 * 17, 100]
-    bufs = [synth.gen(n, synth.MIXED if i == 0 else i, 40 + i) for i, n in enumerate(sizes)]
+    sizes = [40 << 20, 5 << 20, 4128 * 16 + 1, 4128 * 17, 100, 3 << 20]
+    kinds = [synth.MIXED, 1, 2, 3, 4, synth.PERIODIC]
+    bufs = [synth.gen(n, kinds[i], 40 + i) for i, n in enumerate(sizes)]
     outs = {}
     for run in ("32", "16", "5", "1"):
         monkeypatch.setenv("OROT_B200_LAZY_RUN", run)
