@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 #include "engine_host.h"
 #include "geometry_table.h"
+#include "host_copy.h"
 #include "../../include/orot_b200.h"
 
 namespace orotb {
@@ -160,6 +161,8 @@ Engine::Engine() {
 }
 Engine::~Engine() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (made_stage_events)
+    for (cudaEvent_t ev : stage_ev) cudaEventDestroy(ev);
   for (DevBuf* b : {&d_in, &d_out, &d_scratch, &d_tables, &d_pack}) b->release();
   if (stream) cudaStreamSynchronize(stream);
   h_tables.release();
@@ -477,6 +480,31 @@ size_t parallel_bound(size_t n, int fmt, int level, size_t block) {
   return std::max(framed_bound(n, fmt), n + nchunk * (5 * pieces + 1) + 32);
 }
 
+void host_copy(void* dst, const void* src, size_t n) {
+  if (n < (size_t(4) << 20)) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  static std::once_flag once;
+  static CopyPool* pool = nullptr;  // lives until the process exits
+  static std::mutex busy;
+  std::call_once(once, [] {
+    const unsigned hw = std::thread::hardware_concurrency();
+    pool = new CopyPool(int(std::min(8u, std::max(1u, hw / 2))));
+  });
+  std::unique_lock<std::mutex> lk(busy, std::try_to_lock);
+  if (!lk.owns_lock()) {  // another thread's large copy has the copy threads
+    std::memcpy(dst, src, n);
+    return;
+  }
+  pool->run({Copy{static_cast<uint8_t*>(dst), static_cast<const uint8_t*>(src), n}});
+}
+
+// Calls above this many bytes move their input and output in pieces: the
+// host copy of one piece (on the copy threads) overlaps the DMA of another.
+constexpr size_t kPieceStage = size_t(8) << 20;
+constexpr int kStagePieces = 8;
+
 // Pinned staging of a one-call entry point is sized at least this much, so
 // that the first calls do not each grow it (pinning memory is slow).
 constexpr size_t kStageMin = size_t(4) << 20;
@@ -490,9 +518,19 @@ size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, in
   if (!ensure_io(align_up(n, 16), align_up(bound, 16))) return 0;
   if (!h_stage.ensure(std::max({n, bound + 64, kStageMin}))) return 0;
   uint8_t* stage = static_cast<uint8_t*>(h_stage.p);
+  const uint8_t* src = static_cast<const uint8_t*>(in);
   if (n) {
-    std::memcpy(stage, in, n);
-    if (cudaMemcpyAsync(d_in.p, stage, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) { set_error("H2D failed"); return 0; }
+    // in pieces: the copy of piece k + 1 into staging overlaps the DMA of piece k
+    const size_t piece = n < kPieceStage ? n : align_up((n + kStagePieces - 1) / kStagePieces, 4096);
+    for (size_t o = 0; o < n; o += piece) {
+      const size_t len = std::min(piece, n - o);
+      host_copy(stage + o, src + o, len);
+      if (cudaMemcpyAsync(static_cast<uint8_t*>(d_in.p) + o, stage + o, len, cudaMemcpyHostToDevice, stream) !=
+          cudaSuccess) {
+        set_error("H2D failed");
+        return 0;
+      }
+    }
   }
   std::vector<Job> jobs(1);
   jobs[0] = Job{0, n, 0, parallel ? std::min<uint64_t>(cap, bound) : bound, level, fmt, parallel, block, mode};
@@ -507,21 +545,43 @@ size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, in
   }
   if (result) *result = s;
   if (s.error || s.out_size == 0 || s.out_size > cap) return 0;
-  if (!one_trip) {
-    if (cudaMemcpyAsync(stage, static_cast<uint8_t*>(d_out.p) + s.out_off, s.out_size, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-        cudaStreamSynchronize(stream) != cudaSuccess) {
+  uint8_t* dst = static_cast<uint8_t*>(out);
+  if (one_trip) {
+    std::memcpy(dst, stage + s.out_off, s.out_size);
+    return s.out_size;
+  }
+  // in pieces: the copy out of piece k overlaps the DMA of piece k + 1
+  const size_t m = s.out_size;
+  const size_t piece = m < kPieceStage ? m : align_up((m + kStagePieces - 1) / kStagePieces, 4096);
+  if (!made_stage_events) {
+    for (cudaEvent_t& ev : stage_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    made_stage_events = true;
+  }
+  int k = 0;
+  for (size_t o = 0; o < m; o += piece, ++k) {
+    const size_t len = std::min(piece, m - o);
+    if (cudaMemcpyAsync(stage + o, static_cast<uint8_t*>(d_out.p) + s.out_off + o, len, cudaMemcpyDeviceToHost,
+                        stream) != cudaSuccess ||
+        cudaEventRecord(stage_ev[k], stream) != cudaSuccess) {
       set_error("D2H failed");
       return 0;
     }
   }
-  std::memcpy(out, stage + (one_trip ? s.out_off : 0), s.out_size);
+  k = 0;
+  for (size_t o = 0; o < m; o += piece, ++k) {
+    if (cudaEventSynchronize(stage_ev[k]) != cudaSuccess) {
+      set_error("D2H failed");
+      return 0;
+    }
+    host_copy(dst + o, stage + o, std::min(piece, m - o));
+  }
   return s.out_size;
 }
 
 uint32_t Engine::checksum_host(uint32_t init, const void* data, size_t n, bool adler) {
   if (n == 0) return init;
   if (!ensure_io(align_up(n, 16), 64) || !h_stage.ensure(std::max(n, kStageMin))) return init;
-  std::memcpy(h_stage.p, data, n);
+  host_copy(h_stage.p, data, n);
   if (cudaMemcpyAsync(d_in.p, h_stage.p, n, cudaMemcpyHostToDevice, stream) != cudaSuccess) {
     set_error("H2D failed");
     return init;

@@ -107,6 +107,8 @@ class Engine {
   int launches = 0;
   Marks marks;
   bool made_events = false;
+  cudaEvent_t stage_ev[8] = {};  // pieces of an output copied back (compress_host)
+  bool made_stage_events = false;
   void phase_ms(float* ms) const;
 };
 

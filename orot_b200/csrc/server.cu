@@ -28,6 +28,7 @@
 #include <unordered_map>
 #include <vector>
 #include "engine_host.h"
+#include "host_copy.h"
 #include "../../include/orot_b200.h"
 
 namespace orotb {
@@ -156,88 +157,6 @@ static bool lane_warm(Lane& L, uint64_t bytes, int level, uint64_t per_job) {
   while (!lane_poll(L, L.h_out.cap, &failed)) std::this_thread::sleep_for(std::chrono::microseconds(50));
   return !failed;
 }
-
-// Copies between request memory and pinned staging on a few host threads: one
-// memcpy thread moves about 10 GB/s, below what one pass consumes.
-struct Copy {
-  uint8_t* dst;
-  const uint8_t* src;
-  size_t n;
-};
-
-class CopyPool {
- public:
-  explicit CopyPool(int n) {
-    for (int i = 0; i < n; ++i) th_.emplace_back([this] { work(); });
-  }
-  ~CopyPool() {
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      stop_ = true;
-    }
-    cv_.notify_all();
-    for (auto& t : th_) t.join();
-  }
-  // Performs every copy in `v`; returns when all bytes are in place.
-  void run(const std::vector<Copy>& v) {
-    uint64_t total = 0;
-    for (const Copy& c : v) total += c.n;
-    if (th_.empty() || total < kParallelBytes) {
-      for (const Copy& c : v) std::memcpy(c.dst, c.src, c.n);
-      return;
-    }
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      chunks_.clear();
-      for (const Copy& c : v)
-        for (size_t o = 0; o < c.n; o += kChunk) chunks_.push_back({c.dst + o, c.src + o, std::min(kChunk, c.n - o)});
-      next_.store(0);
-      done_.store(0);
-      open_ = true;
-      ++gen_;
-    }
-    cv_.notify_all();
-    drain();
-    while (done_.load(std::memory_order_acquire) < chunks_.size()) std::this_thread::yield();
-    std::unique_lock<std::mutex> lk(mu_);
-    open_ = false;
-    cv_idle_.wait(lk, [this] { return busy_ == 0; });
-  }
-
- private:
-  static constexpr uint64_t kParallelBytes = 4ull << 20;
-  static constexpr size_t kChunk = size_t(1) << 20;
-  void drain() {
-    for (;;) {
-      const size_t i = next_.fetch_add(1);
-      if (i >= chunks_.size()) return;
-      std::memcpy(chunks_[i].dst, chunks_[i].src, chunks_[i].n);
-      done_.fetch_add(1, std::memory_order_release);
-    }
-  }
-  void work() {
-    uint64_t seen = 0;
-    for (;;) {
-      std::unique_lock<std::mutex> lk(mu_);
-      cv_.wait(lk, [&] { return stop_ || (open_ && gen_ != seen); });
-      if (stop_) return;
-      seen = gen_;
-      ++busy_;
-      lk.unlock();
-      drain();
-      lk.lock();
-      if (--busy_ == 0) cv_idle_.notify_all();
-    }
-  }
-  std::vector<std::thread> th_;
-  std::mutex mu_;
-  std::condition_variable cv_, cv_idle_;
-  std::vector<Copy> chunks_;
-  std::atomic<size_t> next_{0}, done_{0};
-  uint64_t gen_ = 0;
-  int busy_ = 0;
-  bool open_ = false, stop_ = false;
-};
 
 // ---------------------------------------------------------------- server
 struct Req {
@@ -551,6 +470,18 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
   if (dst > out_capacity) { set_error("out_capacity below deflate_gpu_packed_bound()"); return 0; }
   const uint8_t* in = static_cast<const uint8_t*>(in_concat);
   uint8_t* out = static_cast<uint8_t*>(out_packed);
+  // Pageable caller memory goes through each lane's pinned buffers, copied by
+  // the copy threads (a DMA from pageable memory is staged by the driver on
+  // one thread); pinned caller memory is read and written by DMA directly.
+  auto pageable = [](const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+      return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+  };
+  const bool stage_in = total && pageable(in), stage_out = pageable(out);
   std::vector<int> lv(count, level), fm(count, int(format));
   std::vector<int> lane_group(nl, -1);
   size_t next = 0, done_groups = 0;
@@ -570,6 +501,7 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
             out_offsets[gfirst[g] + i] = gdst[g] + L.offsets()[i];
             out_sizes[gfirst[g] + i] = L.sizes()[i];
           }
+          if (stage_out) host_copy(out + gdst[g], L.h_out.p, L.total);
           end = std::max<uint64_t>(end, gdst[g] + L.total);
           ++done_groups;
           lane_group[k] = -1;
@@ -578,8 +510,20 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
       if (L.state == 0 && next < gfirst.size()) {
         const size_t g = next++;
         lane_group[k] = int(g);
-        L.dst = out + gdst[g];
-        if (!lane_start(L, in + gsrc[g], in_sizes + gfirst[g], lv.data(), fm.data(), nullptr, gcount[g])) {
+        const uint8_t* gin = in + gsrc[g];
+        const uint64_t gbytes = (g + 1 < gfirst.size() ? gsrc[g + 1] : total) - gsrc[g];
+        if (stage_in) {
+          if (!L.h_in.ensure(std::max<uint64_t>(gbytes, 16))) { ok = false; break; }
+          host_copy(L.h_in.p, gin, gbytes);
+          gin = static_cast<const uint8_t*>(L.h_in.p);
+        }
+        if (stage_out) {
+          if (!L.h_out.ensure(std::max<uint64_t>(gcap[g], 16))) { ok = false; break; }
+          L.dst = static_cast<uint8_t*>(L.h_out.p);
+        } else {
+          L.dst = out + gdst[g];
+        }
+        if (!lane_start(L, gin, in_sizes + gfirst[g], lv.data(), fm.data(), nullptr, gcount[g])) {
           ok = false;
           break;
         }

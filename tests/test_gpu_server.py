@@ -130,3 +130,20 @@ def test_pipelined_batch_equals_single_calls(gpu):
         ref = gpu.compress(b, 1, gpu.Format.Zlib)
         assert szs[i] == len(ref)
         assert out[offs[i]:offs[i] + szs[i]].tobytes() == ref
+
+
+def test_pipelined_batch_pinned_equals_pageable(gpu):
+    """Pageable caller memory is staged through the lanes' pinned buffers;
+    pinned caller memory is read and written by DMA directly: same bytes."""
+    import torch
+    sizes = [int(x) for x in synth.loguniform_sizes(300, 1024, 4 << 20, 8)]
+    concat = np.concatenate([synth.array(n, i % 4, i + 5) for i, n in enumerate(sizes)])
+    bound = gpu.packed_bound(sizes, gpu.Format.Gzip)
+    out_pageable = np.zeros(bound, np.uint8)
+    r1 = gpu.compress_pipelined(concat, sizes, 1, gpu.Format.Gzip, out_pageable, group_bytes=32 << 20, lanes=3)
+    pin_in = torch.from_numpy(concat).pin_memory().numpy()
+    pin_out = torch.zeros(bound, dtype=torch.uint8).pin_memory().numpy()
+    r2 = gpu.compress_pipelined(pin_in, sizes, 1, gpu.Format.Gzip, pin_out, group_bytes=32 << 20, lanes=3)
+    assert r1[0] == r2[0]
+    assert list(r1[1]) == list(r2[1]) and list(r1[2]) == list(r2[2])
+    assert out_pageable[:r1[0]].tobytes() == pin_out[:r2[0]].tobytes()
