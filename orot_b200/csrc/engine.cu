@@ -500,10 +500,15 @@ void host_copy(void* dst, const void* src, size_t n) {
   pool->run({Copy{static_cast<uint8_t*>(dst), static_cast<const uint8_t*>(src), n}});
 }
 
-// Calls above this many bytes move their input and output in pieces: the
-// host copy of one piece (on the copy threads) overlaps the DMA of another.
+// Calls above this many bytes move their input and output in pieces of at
+// least kPieceMin bytes (so that each is copied by the copy threads), at most
+// kStagePieces of them: the host copy of one piece overlaps the DMA of another.
 constexpr size_t kPieceStage = size_t(8) << 20;
+constexpr size_t kPieceMin = size_t(4) << 20;
 constexpr int kStagePieces = 8;
+static size_t stage_piece(size_t n) {
+  return n < kPieceStage ? n : std::max(kPieceMin, align_up((n + kStagePieces - 1) / kStagePieces, 4096));
+}
 
 // Pinned staging of a one-call entry point is sized at least this much, so
 // that the first calls do not each grow it (pinning memory is slow).
@@ -521,7 +526,7 @@ size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, in
   const uint8_t* src = static_cast<const uint8_t*>(in);
   if (n) {
     // in pieces: the copy of piece k + 1 into staging overlaps the DMA of piece k
-    const size_t piece = n < kPieceStage ? n : align_up((n + kStagePieces - 1) / kStagePieces, 4096);
+    const size_t piece = stage_piece(n);
     for (size_t o = 0; o < n; o += piece) {
       const size_t len = std::min(piece, n - o);
       host_copy(stage + o, src + o, len);
@@ -552,7 +557,7 @@ size_t Engine::compress_host(const void* in, size_t n, void* out, size_t cap, in
   }
   // in pieces: the copy out of piece k overlaps the DMA of piece k + 1
   const size_t m = s.out_size;
-  const size_t piece = m < kPieceStage ? m : align_up((m + kStagePieces - 1) / kStagePieces, 4096);
+  const size_t piece = stage_piece(m);
   if (!made_stage_events) {
     for (cudaEvent_t& ev : stage_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     made_stage_events = true;
