@@ -532,6 +532,7 @@ __device__ void cand_tile(const TileView& tv, const uint32_t* carry, uint32_t* s
   const uint32_t nwin = (tv.tl + 31) >> 5;
   uint32_t seg_D = 0, seg_start = 0;  // the run being recorded: its period and first window
   uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
+  uint32_t prevD = 0;  // run period of the previous window (0 = not a run)
   for (uint32_t w = 0; w < nwin; ++w) {
     const uint32_t wpos = tv.ts + (w << 5);
     const uint32_t woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
@@ -539,33 +540,89 @@ __device__ void cand_tile(const TileView& tv, const uint32_t* carry, uint32_t* s
     const uint32_t p = wpos + lane;
     const bool ins = p < tend && p + 4 <= tv.n;
     const uint32_t v4 = wload4(wbuf, woff + lane);
-    const uint32_t h = ins ? hash_fast(v4, HB) : kFull;
-    const uint32_t peers = __match_any_sync(kFull, h);
-    const uint32_t before = peers & lt;
-    const uint32_t src = before ? 31 - __clz(before) : lane;
-    const uint32_t vb = __shfl_sync(kFull, v4, src);
-    uint32_t cpos = 0, cbyte = 0;  // candidate: position mod 32768 | valid bit, first byte
-    if (ins) {
-      if (before) {
-        const uint32_t c = wpos + src;
-        cpos = c ? ((c & 0x7FFFu) | 0x8000u) : 0u;
-        cbyte = vb & 0xFFu;
+    const uint32_t h = ins ? hash_fast(v4, HB) : 0u;
+    const uint32_t mine = p ? ((p & 0x7FFFu) | 0x8000u) : 0u;  // this position as a table entry
+    uint32_t d = 0, runD = 0;  // candidate distance (0 = none), run period of this window
+    uint32_t cpos = 0, cbyte = 0;  // the table's candidate: position mod 32768 | valid bit, first byte
+    bool done = false, have_c = false;
+    // A window that continues the previous window's run of period D (every
+    // position's 4 bytes equal those D earlier) has hashes repeating with
+    // period D.  When the last D lanes' hashes are distinct, every position's
+    // latest same-hash position is the one D earlier and the last D lanes
+    // hold the table's new entries, so the window is done without the
+    // same-hash search.  Period 1 needs no check.
+    if (prevD && __all_sync(kFull, p + 4 <= tend && wload4(wbuf, woff + lane - prevD) == v4)) {
+      const bool top = lane >= 32 - prevD;
+      if (prevD == 1) {
+        done = true;
       } else {
         cpos = head.pos[h];
         cbyte = head.byte[h];
+        have_c = true;
+        __syncwarp();
+        if (top) head.pos[h] = uint16_t(mine);
+        __syncwarp();
+        done = !__any_sync(kFull, top && head.pos[h] != mine);
+      }
+      if (done) {
+        if (prevD == 1 && top) head.pos[h] = uint16_t(mine);
+        if (top) head.byte[h] = uint8_t(v4);
+        d = prevD;
+        runD = prevD;
       }
     }
-    __syncwarp();
-    if (ins && (peers >> lane) == 1u) head.put(h, p, v4 & 0xFFu);
-    uint32_t d = 0;
-    if (cpos & 0x8000u) {
-      const uint32_t dist = (p - (cpos & 0x7FFFu)) & 0x7FFFu;
-      if (dist != 0 && cbyte == (v4 & 0xFFu)) d = dist;
+    if (!done) {
+      // the table's candidate (the latest position of the hash in earlier
+      // windows), read before any entry of this window is stored
+      if (!have_c) {
+        cpos = ins ? head.pos[h] : 0u;
+        cbyte = ins ? head.byte[h] : 0u;
+        __syncwarp();
+      }
+      // Every lane stores its position and reads the entry back.  Positions
+      // differ, so all read back their own exactly when no two lanes of the
+      // window share a hash; only then may the table's candidate stand for
+      // every lane and every lane's entry stay.  Otherwise (repeats within
+      // 32 bytes) the lanes of each hash are found with __match_any_sync,
+      // whose cost grows with the number of distinct hashes in the warp: the
+      // nearest earlier lane is the candidate and the last lane's entry
+      // stays.  After a run window (repeats all but certain) the probe is
+      // skipped.
+      bool clash = true, last = ins;
+      if (!prevD && !have_c) {
+        if (ins) head.pos[h] = uint16_t(mine);
+        __syncwarp();
+        clash = __any_sync(kFull, ins && head.pos[h] != mine);
+      }
+      if (clash) {
+        const uint32_t peers = __match_any_sync(kFull, ins ? h : kFull);
+        const uint32_t before = peers & lt;
+        const uint32_t src = before ? 31 - __clz(before) : lane;
+        const uint32_t vb = __shfl_sync(kFull, v4, src);
+        if (ins && before) {
+          const uint32_t c = wpos + src;
+          cpos = c ? ((c & 0x7FFFu) | 0x8000u) : 0u;
+          cbyte = vb & 0xFFu;
+        }
+        last = ins && (peers >> lane) == 1u;
+        __syncwarp();
+        if (last) head.pos[h] = uint16_t(mine);
+      }
+      if (last) head.byte[h] = uint8_t(v4);
+      // candidate distance after the first-byte check at the candidate itself
+      if (cpos & 0x8000u) {
+        const uint32_t dist = (p - (cpos & 0x7FFFu)) & 0x7FFFu;
+        if (dist != 0 && cbyte == (v4 & 0xFFu)) d = dist;
+      }
+      // run window: every position has the same distance D <= 32 and its
+      // four bytes equal the four bytes D earlier (checked only when every
+      // lane has a distance of at most 32)
+      if (wpos >= 32 && __all_sync(kFull, d != 0 && d <= 32 && p + 4 <= tend)) {
+        const uint32_t D = __shfl_sync(kFull, d, 0);
+        runD = __all_sync(kFull, d == D && wload4(wbuf, woff + lane - D) == v4) ? D : 0u;
+      }
     }
     if (p < tend) cand16[p - tv.ts] = uint16_t(d);
-    const uint32_t D = __shfl_sync(kFull, d, 0);
-    const bool ok = wpos >= 32 && D != 0 && D <= 32 && d == D && p + 4 <= tend && wload4(wbuf, woff + lane - D) == v4;
-    const uint32_t runD = __ballot_sync(kFull, ok) == kFull ? D : 0u;
     // consecutive run windows of one period form a run; when it ends, each of
     // its windows records the period and the window after the run, so the
     // fix-up crosses a run without scanning it
@@ -575,8 +632,8 @@ __device__ void cand_tile(const TileView& tv, const uint32_t* carry, uint32_t* s
       seg_D = runD;
       seg_start = w;
     }
+    prevD = runD;
     if (!runD && lane == 0) rec[w].run = 0;
-    __syncwarp();
   }
   if (seg_D)
     for (uint32_t k = seg_start + lane; k < nwin; k += 32) rec[k].run = seg_D | (nwin << 8);
