@@ -82,8 +82,8 @@ HBM_FALLBACK_GBS = 6650.0
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) on a slice of
 # this workload; every term of that traffic is per byte or per tile, so it is
 # scaled by the input size for the full launch (profiles/k_cand_k_parse_L1_mixed_300MB.md).
-DRAM_BYTES_PER_INPUT_BYTE = {"candidates": (759.291e6 + 702.074e6) / 301540590,
-                             "parse": (1320.586e6 + 340.746e6) / 301540590}
+DRAM_BYTES_PER_INPUT_BYTE = {"candidates": (759.450e6 + 703.093e6) / 301540590,
+                             "parse": (1321.767e6 + 341.029e6) / 301540590}
 
 
 def parse():
@@ -464,7 +464,7 @@ def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
 # ---------------------------------------------------------------- the other configurations
 # ncu figures of the two dominant kernels (profiles/): warp instructions per
 # input byte, for the issue-rate roofline (4 warp instructions per SM cycle).
-WARP_INST_PER_BYTE = {"candidates": 3.75, "parse": 8.56, "lazy_match": 79.3}
+WARP_INST_PER_BYTE = {"candidates": 3.65, "parse": 8.56, "lazy_match": 79.3}
 PHASE_KERNEL = {"candidates": "k_cand", "parse": "k_parse", "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
                 "hash_carry": "k_lastocc + k_carry_scan", "fixup": "k_fix1 + k_fix2", "join": "k_join",
                 "checksum": "k_ck_block + k_ck_fold", "plan": "k_plan + k_zero"}

@@ -13,8 +13,9 @@
 //   k_carry_scan  per segment, exclusive prefix-max of those tables
 //   k_cand        one warp per tile, head[] in shared memory (18 walkers of
 //                 12.4 KB per SM at 12 hash bits): 32 positions per step;
-//                 hash, __match_any for same-hash lanes, head lookup and
-//                 insert; the candidate distance of every position (2 bytes)
+//                 hash, head lookup, insert by store and read-back (a
+//                 window with a repeated hash groups its lanes with
+//                 __match_any); the candidate distance of every position (2 bytes)
 //                 and the run period of every 32-position window.
 //   k_parse       one warp per tile, no table (16 warps of 0.6 KB per CTA,
 //                 two CTAs per SM): capped match lengths per lane, greedy
