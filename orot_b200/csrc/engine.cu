@@ -365,6 +365,8 @@ bool Engine::plan(const std::vector<Job>& jobs) {
   for (int i = 0; i < kNumLists; ++i) off_lists[i] = put_table(buf, lists[i]);
   off_counters = align_up(buf.size(), 256);
   buf.resize(off_counters + 256, 0);
+  off_ready = align_up(buf.size(), 256);
+  buf.resize(off_ready + 4 * (lists[kWalk12].size() + lists[kWalk14].size()), 0);
   off_pieces = align_up(buf.size(), 256);
   const uint64_t table_bytes = off_pieces + uint64_t(npieces) * sizeof(Piece) + 256;
   if (!d_tables.ensure(table_bytes) || !h_tables.ensure(buf.size())) return false;
@@ -416,11 +418,13 @@ bool Engine::launch(cudaStream_t st) {
     L.n_multi = uint32_t(lists[g ? kMulti14 : kMulti12].size());
     L.walk = list(g ? kWalk14 : kWalk12);
     L.n_walk = uint32_t(lists[g ? kWalk14 : kWalk12].size());
-    L.counter = counters + g;  // candidates: 0/1; fix-up round 1: 4/5 (+ 4); parse: 6/7 (+ 6)
+    L.counter = counters + g;  // candidates: 0/1; fix-up round 1: 4/5 (+ 4); parse: 6/7 (+ 6); abort: 12/13 (+ 12)
+    L.ready = reinterpret_cast<uint32_t*>(t + off_ready) + (g ? lists[kWalk12].size() : 0);
     if (L.n_walk) {
       launch_fast(w, L, hbs[g], st, sms, &marks);
-      // k_lastocc; k_carry_scan, k_fix1, k_fix2 for multi-tile segments; k_cand, k_parse
-      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 3 : 0) + 2;
+      // k_lastocc; k_carry_scan, k_fix1, k_fix2 for multi-tile segments;
+      // k_cand_parse (or k_cand and k_parse)
+      launches += (L.n_lastocc ? 1 : 0) + (L.n_multi ? 3 : 0) + (fast_launches_fused() ? 1 : 2);
     }
   }
   if (!lists[kLazyTiles].empty()) {

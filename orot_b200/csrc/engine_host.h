@@ -103,6 +103,7 @@ class Engine {
   uint64_t scratch_bytes = 0, upload_bytes = 0;
   uint64_t max_out_cap = 0;  // largest output slot of the planned pass
   uint64_t off_streams = 0, off_segs = 0, off_tiles = 0, off_ck = 0, off_pieces = 0, off_counters = 0;
+  uint64_t off_ready = 0;  // per fast-level tile: candidates done (zeroed by every upload)
   uint64_t off_lists[kNumLists] = {};
   int launches = 0;
   Marks marks;

@@ -39,7 +39,8 @@ struct FastLists {
   uint32_t n_multi;
   const uint32_t* walk;      // tiles to walk
   uint32_t n_walk;
-  uint32_t* counter;         // zeroed work counter for k_walk
+  uint32_t* counter;         // zeroed work counters
+  uint32_t* ready;           // zeroed, one flag per tile of `walk` (candidates done)
 };
 
 // Index lists for the lazy-level (4-12) pipeline.
@@ -69,6 +70,8 @@ struct Marks {
 };
 
 void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms, Marks* mk);
+// Whether launch_fast runs the candidate pass and the parse as one kernel.
+bool fast_launches_fused();
 int launch_lazy(const Work& wk, const LazyLists& L, cudaStream_t st, int sms, Marks* mk);
 void launch_plan(const Work& wk, uint64_t max_out, cudaStream_t st);  // max_out: largest stream bound
 void launch_checksums(const Work& wk, cudaStream_t st);

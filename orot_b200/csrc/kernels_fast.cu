@@ -32,6 +32,7 @@
 // The output is therefore token-for-token the reference's.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <cstdlib>
 #include "engine.cuh"
 #include "deflate_device.cuh"
 #include "kernels.cuh"
@@ -150,14 +151,14 @@ __device__ __forceinline__ uint32_t wload4(const uint32_t* wbuf, uint32_t off) {
 }
 
 // Capped common-prefix length of the bytes at p (staged at wbuf offset po)
-// and at q (global), at most cap <= kCapMax.  The first 8 q-side words are
-// loaded in one batch (one memory latency covers matches up to ~24 bytes);
+// and at q (global), at most cap <= kCapMax.  The first 4 q-side words are
+// loaded in one batch (one memory latency covers matches up to ~12 bytes);
 // longer matches fetch one more word per step.  The loop runs while any lane
 // of the warp is still matching, so its trip count follows the longest match
 // in the window rather than the cap.  Every lane of the warp must call it.
 __device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_t* wbuf, uint32_t po, uint32_t q,
                                                uint32_t cap, bool active) {
-  constexpr int PRE = 8;
+  constexpr int PRE = 4;
   const uint32_t qa = q + sb.boff;
   const uint32_t* qw = sb.w + (qa >> 2);
   const uint32_t qs = (qa & 3) * 8;
@@ -172,13 +173,12 @@ __device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_
 #pragma unroll
   for (int j = 0; j < PRE - 1; ++j) {
     if (!__any_sync(kFull, open)) break;
-    if (open) {
-      const uint32_t phi = pw[j + 1];
-      const uint32_t x = __funnelshift_r(plo, phi, ps) ^ __funnelshift_r(v[j], v[j + 1], qs);
-      plo = phi;
-      if (x) { n += (__ffs(x) - 1) >> 3; open = false; } else { n += 4; }
-      if (n >= cap) open = false;
-    }
+    // staged words (po >> 2) + j + 1 <= 23 < kWbuf: in bounds for every lane
+    const uint32_t phi = pw[j + 1];
+    const uint32_t x = __funnelshift_r(plo, phi, ps) ^ __funnelshift_r(v[j], v[j + 1], qs);
+    plo = phi;
+    n += open ? (x ? (__ffs(x) - 1) >> 3 : 4u) : 0u;
+    open = open && !x && n < cap;
   }
   uint32_t lo = v[PRE - 1];
   for (uint32_t j = PRE - 1; __any_sync(kFull, open); ++j) {
@@ -197,11 +197,22 @@ __device__ __forceinline__ uint32_t lcp_window(const SegBytes& sb, const uint32_
 
 // Fixed-Huffman code tables for the parse kernels: literal b at [b], match
 // length L (3..258) at [256 + L]; each entry is the LSB-first bits | count << 16
-// (a length entry holds the length symbol and its extra bits).
-constexpr uint32_t kCodeTab = 256 + 259;
+// (a length entry holds the length symbol and its extra bits).  Distance
+// codes at [kDistTab + (d - 1)] for d - 1 < 256, else at
+// [kDistTab + 256 + ((d - 1) >> 7)] (the code of a larger distance depends only
+// on its bits above the 7th): the 5-bit code reversed | extra-bit count << 8.
+constexpr uint32_t kDistTab = 256 + 259;
+constexpr uint32_t kCodeTab = kDistTab + 512;
 __device__ __forceinline__ void fill_code_tab(uint32_t* tab) {
   for (uint32_t i = threadIdx.x; i < kCodeTab; i += blockDim.x) {
     uint32_t bits = 0, nb = 0;
+    if (i >= kDistTab) {
+      const uint32_t t = i - kDistTab, dm1 = t < 256 ? t : (t - 256) << 7;
+      uint32_t dc, de, dv;
+      dist_code(dm1 + 1, dc, de, dv);
+      tab[i] = rev_bits(dc, 5) | (de << 8);
+      continue;
+    }
     if (i < 256) {
       fixed_literal(i, bits, nb);
     } else if (i >= 256 + 3) {
@@ -218,12 +229,13 @@ __device__ __forceinline__ void fill_code_tab(uint32_t* tab) {
 __device__ __forceinline__ void tab_match(const uint32_t* tab, uint32_t len, uint32_t dist, uint32_t& bits,
                                           uint32_t& nb) {
   const uint32_t t = tab[256 + len];
-  uint32_t dc, de, dv;
-  dist_code(dist, dc, de, dv);
-  bits = (t & 0xFFFFu) | (rev_bits(dc, 5) << (t >> 16));
+  const uint32_t dm1 = dist - 1;
+  const uint32_t e = tab[kDistTab + (dm1 < 256 ? dm1 : 256 + (dm1 >> 7))];
+  const uint32_t ne = e >> 8;
+  bits = (t & 0xFFFFu) | ((e & 31u) << (t >> 16));
   nb = (t >> 16) + 5;
-  bits |= dv << nb;
-  nb += de;
+  bits |= (dm1 & ((1u << ne) - 1u)) << nb;
+  nb += ne;
 }
 
 // head[] entry: the candidate's position mod 32768 with a valid bit (u16)
@@ -304,16 +316,20 @@ __device__ __forceinline__ void parse_window(const SegBytes& sb, uint32_t n, uin
   const bool vis = (visited >> lane) & 1u;
   const bool ism = vis && ((M >> lane) & 1u);
   uint32_t code = 0, nb = 0;
-  if (vis) {
-    if (ctab) {
-      if (ism) {
-        tab_match(ctab, int(lane) == xl ? full : clen, d, code, nb);
-      } else {
-        const uint32_t t = ctab[wload4(wbuf, woff + lane) & 0xFFu];
-        code = t & 0xFFFFu;
-        nb = t >> 16;
-      }
-    } else if (ism) {
+  if (ctab) {
+    if (visited & M) {  // a match in the window: both codes, selected per lane
+      uint32_t mc, mn;
+      tab_match(ctab, ism ? (int(lane) == xl ? full : clen) : 3u, ism ? d : 1u, mc, mn);
+      const uint32_t t = ctab[wload4(wbuf, woff + lane) & 0xFFu];
+      code = !vis ? 0u : ism ? mc : (t & 0xFFFFu);
+      nb = !vis ? 0u : ism ? mn : (t >> 16);
+    } else if (vis) {
+      const uint32_t t = ctab[wload4(wbuf, woff + lane) & 0xFFu];
+      code = t & 0xFFFFu;
+      nb = t >> 16;
+    }
+  } else if (vis) {
+    if (ism) {
       fixed_match(int(lane) == xl ? full : clen, d, code, nb);
     } else {
       fixed_literal(wload4(wbuf, woff + lane) & 0xFFu, code, nb);
@@ -667,7 +683,63 @@ __global__ void __launch_bounds__(WARPS * 32) k_cand(Work wk, const uint32_t* __
 // candidates: greedy parse, fixed-Huffman bits, and per window the parse
 // entry, bit offset and match count for the fix-up.  Windows that a match
 // covers entirely cost only that record.  Shared memory per warp is the bit
-// ring and the staged bytes, so many warps share an SM.
+// ring and the staged bytes, so many warps share an SM.  The candidates are
+// read at L2 (ld.global.cg): in the fused kernel they were written by other
+// SMs during the same launch.
+__device__ void parse_tile(const Work& wk, Tile* tp, uint32_t* ring, uint32_t* wbuf, const uint32_t* ctab) {
+  const uint32_t lane = threadIdx.x & 31;
+  const Tile t = *tp;
+  const Segment sg = wk.segs[t.seg];
+  const TileView tv = tile_view(wk, t, sg);
+  WinRec* rec = reinterpret_cast<WinRec*>(wk.scratch + t.rec);
+  const uint16_t* c16 = reinterpret_cast<const uint16_t*>(wk.scratch + t.cand);
+  uint32_t* out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch);
+  for (uint32_t k = lane; k < kRing; k += 32) ring[k] = 0;
+  __syncwarp();
+  WinState st{tv.ts, 0, 0, 0, 0};
+  const uint32_t tend = tv.ts + tv.tl;
+  const uint32_t nwin = (tv.tl + 31) >> 5;
+  // the next window's bytes and candidates are loaded one window ahead
+  uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
+  uint32_t dnext = lane < tv.tl ? __ldcg(c16 + lane) : 0u;
+  uint32_t pre_w = 0;
+  for (uint32_t w = 0; w < nwin; ++w) {
+    const uint32_t wpos = tv.ts + (w << 5);
+    const uint32_t lim = min(32u, tend - wpos);
+    // parse state where the parse enters this window (lanes 0-2 write one field each)
+    const uint32_t f = lane == 0 ? st.np - tv.ts : lane == 1 ? st.cursor : st.matches;
+    if (lane < 3) reinterpret_cast<uint32_t*>(rec + w)[lane] = f;
+    if (st.np >= wpos + lim) continue;  // covered by a match
+    uint32_t woff, d;
+    if (pre_w == w) {
+      woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
+      d = dnext;
+    } else {
+      woff = stage_window(tv.sb, wpos, wbuf, lane, prefetch_window(tv.sb, wpos, lane));
+      d = lane < lim ? __ldcg(c16 + (w << 5) + lane) : 0u;
+    }
+    if (w + 1 < nwin) {
+      pre = prefetch_window(tv.sb, wpos + 32, lane);
+      const uint32_t q = ((w + 1) << 5) + lane;
+      dnext = q < tv.tl ? __ldcg(c16 + q) : 0u;
+      pre_w = w + 1;
+    }
+    parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st, ctab);
+  }
+  flush_tail(ring, out, st, lane);
+  if (lane == 0) {
+    tp->spec_bits = st.cursor;
+    tp->spec_matches = st.matches;
+    tp->spec_exit = st.np;
+    tp->spec_tokens = st.tokens;
+    tp->fix_bits = 0;
+    tp->splice_bit = 0;
+    tp->fin_matches = st.matches;
+    tp->fin_exit = st.np;
+    tp->fix_entry = t.start;
+  }
+}
+
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, 2) k_parse(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
                                                           uint32_t* __restrict__ counter) {
@@ -683,57 +755,114 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_parse(Work wk, const uint32_t
     if (lane == 0) i = atomicAdd(counter, 1u);
     i = __shfl_sync(kFull, i, 0);
     if (i >= nlist) break;
+    parse_tile(wk, wk.tiles + list[i], ring, wbuf, ctab);
+  }
+}
+
+// ---------------------------------------------------------------- k_cand_parse
+// The candidate pass and the parse in one persistent kernel, one CTA of 32
+// warps per SM: the first CW warps are candidate walkers (head tables in
+// shared memory), the others parse, and a walker whose candidate work is
+// exhausted parses too.  Walkers take tiles in list order and publish each
+// finished tile in `ready`; parsers take tiles in the same order and wait for
+// its flag.  The two kinds of warp have complementary limits (walkers:
+// shared-memory and warp-collective latency; parsers: instruction issue), so
+// an SM running both issues more than it does running either alone.  A walker
+// never waits, so every flag a parser waits for is set by a running warp; the
+// wait is bounded all the same (kReadyWaitNs; the first parser that gives up
+// makes every later wait of the launch give up at once), and a parser that
+// gives up marks the tile's segment failed and leaves the tile as empty.
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t fast_global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr uint64_t kReadyWaitNs = 1000000000ull;
+// Waits for `flag`; false after kReadyWaitNs, or at once when another
+// parser of the launch has already given up (`abort`, which it then sets).
+__device__ __noinline__ bool wait_ready(const uint32_t* flag, uint32_t* abort) {
+  if (ld_acquire_gpu(flag)) return true;
+  const uint64_t t0 = fast_global_ns();
+  uint32_t nap = 64;
+  for (;;) {
+    __nanosleep(nap);
+    if (nap < 2048) nap <<= 1;
+    if (ld_acquire_gpu(flag)) return true;
+    if (*reinterpret_cast<volatile uint32_t*>(abort) || fast_global_ns() - t0 > kReadyWaitNs) {
+      atomicExch(abort, 1u);
+      return false;
+    }
+  }
+}
+template <int HB>
+__host__ __device__ constexpr uint32_t cand_parse_words(int cw) {
+  return kCodeTab + uint32_t(cw) * (((1u << HB) * 3 + 3) / 4 + kWbuf) + uint32_t(32 - cw) * (kRing + kWbuf);
+}
+template <int HB, int CW>
+__global__ void __launch_bounds__(1024, 1) k_cand_parse(Work wk, const uint32_t* __restrict__ list, uint32_t nlist,
+                                                         uint32_t* __restrict__ counter, uint32_t* __restrict__ ready) {
+  extern __shared__ uint32_t sm[];
+  constexpr uint32_t HW = ((1u << HB) * 3 + 3) / 4;
+  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t* ctab = sm;
+  uint32_t* own = wid < CW ? sm + kCodeTab + wid * (HW + kWbuf)
+                           : sm + kCodeTab + CW * (HW + kWbuf) + (wid - CW) * (kRing + kWbuf);
+  fill_code_tab(ctab);
+  __syncthreads();
+  if (wid < CW) {
+    for (;;) {
+      uint32_t i = 0;
+      if (lane == 0) i = atomicAdd(counter, 1u);
+      i = __shfl_sync(kFull, i, 0);
+      if (i >= nlist) break;
+      const Tile t = wk.tiles[list[i]];
+      const Segment sg = wk.segs[t.seg];
+      const TileView tv = tile_view(wk, t, sg);
+      const uint32_t* carry = t.index ? reinterpret_cast<const uint32_t*>(wk.scratch + t.carry) : nullptr;
+      cand_tile<HB>(tv, carry, own, own + HW, reinterpret_cast<WinRec*>(wk.scratch + t.rec),
+                    reinterpret_cast<uint16_t*>(wk.scratch + t.cand));
+      __threadfence();  // this lane's candidates and records, before the flag
+      __syncwarp();
+      if (lane == 0) st_release_gpu(ready + i, 1u);
+    }
+  }
+  uint32_t* ring = own;  // a walker's head-table space holds a parser's ring and staged bytes
+  uint32_t* wbuf = own + kRing;
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(counter + 6, 1u);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= nlist) break;
     Tile* tp = wk.tiles + list[i];
-    const Tile t = *tp;
-    const Segment sg = wk.segs[t.seg];
-    const TileView tv = tile_view(wk, t, sg);
-    WinRec* rec = reinterpret_cast<WinRec*>(wk.scratch + t.rec);
-    const uint16_t* c16 = reinterpret_cast<const uint16_t*>(wk.scratch + t.cand);
-    uint32_t* out = reinterpret_cast<uint32_t*>(wk.scratch + t.scratch);
-    for (uint32_t k = lane; k < kRing; k += 32) ring[k] = 0;
+    uint32_t ok = 1;
+    if (lane == 0) ok = wait_ready(ready + i, counter + 12) ? 1u : 0u;
+    ok = __shfl_sync(kFull, ok, 0);
     __syncwarp();
-    WinState st{tv.ts, 0, 0, 0, 0};
-    const uint32_t tend = tv.ts + tv.tl;
-    const uint32_t nwin = (tv.tl + 31) >> 5;
-    // the next window's bytes and candidates are loaded one window ahead
-    uint32_t pre = prefetch_window(tv.sb, tv.ts, lane);
-    uint32_t dnext = lane < tv.tl ? c16[lane] : 0u;
-    uint32_t pre_w = 0;
-    for (uint32_t w = 0; w < nwin; ++w) {
-      const uint32_t wpos = tv.ts + (w << 5);
-      const uint32_t lim = min(32u, tend - wpos);
-      // parse state where the parse enters this window (lanes 0-2 write one field each)
-      const uint32_t f = lane == 0 ? st.np - tv.ts : lane == 1 ? st.cursor : st.matches;
-      if (lane < 3) reinterpret_cast<uint32_t*>(rec + w)[lane] = f;
-      if (st.np >= wpos + lim) continue;  // covered by a match
-      uint32_t woff, d;
-      if (pre_w == w) {
-        woff = stage_window(tv.sb, wpos, wbuf, lane, pre);
-        d = dnext;
-      } else {
-        woff = stage_window(tv.sb, wpos, wbuf, lane, prefetch_window(tv.sb, wpos, lane));
-        d = lane < lim ? c16[(w << 5) + lane] : 0u;
+    if (!ok) {
+      if (lane == 0) {
+        atomicOr(&wk.segs[tp->seg].flags, kSegFault);
+        tp->spec_bits = 0;
+        tp->spec_matches = 0;
+        tp->spec_exit = tp->start + tp->len;
+        tp->spec_tokens = 0;
+        tp->fix_bits = 0;
+        tp->splice_bit = 0;
+        tp->fin_matches = 0;
+        tp->fin_exit = tp->start + tp->len;
+        tp->fix_entry = tp->start;
       }
-      if (w + 1 < nwin) {
-        pre = prefetch_window(tv.sb, wpos + 32, lane);
-        const uint32_t q = ((w + 1) << 5) + lane;
-        dnext = q < tv.tl ? c16[q] : 0u;
-        pre_w = w + 1;
-      }
-      parse_window(tv.sb, tv.n, wpos, lim, lane, wbuf, woff, d, ring, out, st, ctab);
+      __syncwarp();
+      continue;
     }
-    flush_tail(ring, out, st, lane);
-    if (lane == 0) {
-      tp->spec_bits = st.cursor;
-      tp->spec_matches = st.matches;
-      tp->spec_exit = st.np;
-      tp->spec_tokens = st.tokens;
-      tp->fix_bits = 0;
-      tp->splice_bit = 0;
-      tp->fin_matches = st.matches;
-      tp->fin_exit = st.np;
-      tp->fix_entry = t.start;
-    }
+    parse_tile(wk, tp, ring, wbuf, ctab);
   }
 }
 
@@ -827,6 +956,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_fix2(Work wk, const uint32_t* __
 }
 
 // ---------------------------------------------------------------- launchers
+// The fused candidate + parse kernel is the default; OROT_B200_FUSED=0 runs
+// the two passes as separate kernels (same bytes).
+static bool fused_cand_parse() {
+  static const bool on = [] {
+    const char* e = getenv("OROT_B200_FUSED");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 template <int HB>
 static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, int sms, Marks* mk) {
   constexpr int H = 1 << HB;
@@ -855,7 +993,21 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
     k_carry_scan<HB><<<g, 256, 0, st>>>(wk, L.multi, L.n_multi);
   }
   mk->mark(kPhPre, st);
-  if (L.n_walk) {
+  if (L.n_walk && L.ready && fused_cand_parse()) {
+    // one persistent CTA per SM: CW walkers and 32 - CW parsers
+    constexpr int CW = HB <= 12 ? 16 : 4;
+    const size_t fsm = size_t(cand_parse_words<HB>(CW)) * 4;
+    static std::atomic<int> fused_attr[64];
+    if (!fused_attr[ds].load(std::memory_order_relaxed)) {
+      cudaFuncSetAttribute(k_cand_parse<HB, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fsm));
+      fused_attr[ds].store(1, std::memory_order_relaxed);
+    }
+    uint32_t blocks = uint32_t(sms);
+    const uint32_t need = (L.n_walk + CW - 1) / CW;
+    if (blocks > need) blocks = need;
+    mk->mark(kPhCand, st);
+    k_cand_parse<HB, CW><<<blocks, 1024, fsm, st>>>(wk, L.walk, L.n_walk, L.counter, L.ready);
+  } else if (L.n_walk) {
     uint32_t blocks = uint32_t(per_sm) * uint32_t(sms);
     const uint32_t need = (L.n_walk + WARPS - 1) / WARPS;
     if (blocks > need) blocks = need;
@@ -885,6 +1037,8 @@ static void launch_fast_t(const Work& wk, const FastLists& L, cudaStream_t st, i
   }
   mk->mark(kPhFix, st);
 }
+
+bool fast_launches_fused() { return fused_cand_parse(); }
 
 void launch_fast(const Work& wk, const FastLists& L, int hash_bits, cudaStream_t st, int sms, Marks* mk) {
   if (hash_bits == 12) launch_fast_t<12>(wk, L, st, sms, mk);

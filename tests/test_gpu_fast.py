@@ -170,13 +170,43 @@ def test_device_batch_equals_single_calls(gpu):
 def test_launch_count_matches_the_kernels_of_a_pass(gpu):
     """deflate_gpu_batch_launches counts every kernel of a pass: at level 1
     with a multi-tile buffer and zlib framing that is k_lastocc, k_carry_scan,
-    k_cand, k_parse, k_fix1, k_fix2, k_plan_seg, k_plan_stream,
-    k_plan_pieces, k_zero, k_join, k_ck_block, k_ck_fold and k_frame (14);
-    raw output drops the two checksum kernels."""
+    k_cand_parse (the candidate pass and the parse in one kernel), k_fix1,
+    k_fix2, k_plan_seg, k_plan_stream, k_plan_pieces, k_zero, k_join,
+    k_ck_block, k_ck_fold and k_frame (13); raw output drops the two checksum
+    kernels."""
     d = synth.gen(3 << 20, synth.MIXED, 2)
-    for fmt, want in ((gpu.Format.Zlib, 14), (gpu.Format.Raw, 12)):
+    for fmt, want in ((gpu.Format.Zlib, 13), (gpu.Format.Raw, 11)):
         b = gpu.DeviceBatch()
         b.load(d, [len(d)], 1, fmt)
         b.run()
         assert b.launches() == want
         b.close()
+
+
+_FUSED_CASES = "[(k, n, lv) for k, n in ((0, 3 << 20), (2, 1 << 20), (4, 5 << 20), (5, 700001), (1, 2 << 20)) for lv in (1, 2, 3)]"
+_FUSED_SCRIPT = """
+import hashlib, sys
+sys.path.insert(0, {root!r})
+from orot_b200 import deflate, synth
+for k, n, lv in {cases}:
+    print(hashlib.sha256(deflate.compress(synth.gen(n, k, 31 + k), lv, deflate.Format.Raw)).hexdigest())
+"""
+
+
+def test_fused_and_separate_kernels_same_bytes(gpu):
+    """The candidate pass and the parse run as one kernel (k_cand_parse) by
+    default; OROT_B200_FUSED=0 runs them as k_cand then k_parse.  Both give
+    the same bytes at every fast level, multi-tile buffers included."""
+    import hashlib
+    import os
+    import subprocess
+    import sys
+    cases = eval(_FUSED_CASES)
+    fused = [hashlib.sha256(gpu.compress(synth.gen(n, k, 31 + k), lv, gpu.Format.Raw)).hexdigest()
+             for k, n, lv in cases]
+    root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+    env = dict(os.environ, OROT_B200_FUSED="0")
+    p = subprocess.run([sys.executable, "-c", _FUSED_SCRIPT.format(root=root, cases=_FUSED_CASES)], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.split() == fused
