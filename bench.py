@@ -81,9 +81,9 @@ HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per input byte of the dominant kernel, from one
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) on a slice of
 # this workload; every term of that traffic is per byte or per tile, so it is
-# scaled by the input size for the full launch (profiles/k_cand_k_parse_L1_mixed_300MB.md).
+# scaled by the input size for the full launch (profiles/k_cand_parse_L1_mixed_300MB.md).
 DRAM_BYTES_PER_INPUT_BYTE = {"candidates": (759.450e6 + 703.093e6) / 301540590,
-                             "parse": (1321.767e6 + 341.029e6) / 301540590}
+                             "parse": (2088.913e6 + 1095.331e6) / 301540590}
 
 
 def parse():
@@ -462,10 +462,12 @@ def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
 
 
 # ---------------------------------------------------------------- the other configurations
-# ncu figures of the two dominant kernels (profiles/): warp instructions per
+# ncu figures of the dominant kernels (profiles/): warp instructions per
 # input byte, for the issue-rate roofline (4 warp instructions per SM cycle).
-WARP_INST_PER_BYTE = {"candidates": 3.65, "parse": 8.56, "lazy_match": 79.3}
-PHASE_KERNEL = {"candidates": "k_cand", "parse": "k_parse", "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
+# The "parse" phase is k_cand_parse, the candidate pass and the parse in one
+# kernel (the "candidates" phase is empty then).
+WARP_INST_PER_BYTE = {"candidates": 3.65, "parse": 12.07, "lazy_match": 79.3}
+PHASE_KERNEL = {"candidates": "k_cand", "parse": "k_cand_parse",  "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
                 "hash_carry": "k_lastocc + k_carry_scan", "fixup": "k_fix1 + k_fix2", "join": "k_join",
                 "checksum": "k_ck_block + k_ck_fold", "plan": "k_plan + k_zero"}
 
