@@ -44,7 +44,7 @@ constexpr uint32_t kFull = 0xFFFFFFFFu;
 __device__ __forceinline__ uint32_t hash_fast(uint32_t v, int hb) { return (v * 0x9E3779B1u) >> (32 - hb); }
 
 // ---------------------------------------------------------------- k_lastocc
-// Each thread hashes 16 consecutive positions from 6 loaded words; a position
+// Each thread hashes 16 consecutive positions from 5 loaded words; a position
 // followed by one with the same hash (runs) needs no atomic, since the later
 // position wins the max anyway.
 template <int HB>
@@ -61,25 +61,24 @@ __global__ void __launch_bounds__(256) k_lastocc(Work wk, const uint32_t* __rest
   const uint32_t boff = uint32_t(a & 3);
   const uint32_t end = t.start + t.len;
   const uint32_t lim = sg.len >= 4 ? min(end, sg.len - 3) : t.start;  // positions with 4 bytes
-  for (uint32_t base = t.start + 16 * threadIdx.x; base < lim; base += 16 * blockDim.x) {
-    const uint32_t q = base + boff;
-    const uint32_t* qw = w + (q >> 2);
-    const uint32_t sh = q & 3;
-    uint32_t W[6];
+  // 16 positions per thread from word-aligned loads: the byte offsets of the
+  // funnel shifts are then constants.  Positions before the tile start or
+  // without 4 bytes are masked.
+  const uint32_t q0 = (t.start + boff) & ~3u;
+  for (uint32_t qb = q0 + 16 * threadIdx.x; qb < lim + boff; qb += 16 * blockDim.x) {
+    const uint32_t* qw = w + (qb >> 2);
+    uint32_t W[5];
 #pragma unroll
-    for (int j = 0; j < 6; ++j) W[j] = __ldg(qw + j);
+    for (int j = 0; j < 5; ++j) W[j] = __ldg(qw + j);
     uint32_t h[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const uint32_t k = sh + i;
-      h[i] = hash_fast(__funnelshift_r(W[k >> 2], W[(k >> 2) + 1], (k & 3) * 8), HB);
-    }
+    for (int i = 0; i < 16; ++i) h[i] = hash_fast(__funnelshift_r(W[i >> 2], W[(i >> 2) + 1], (i & 3) * 8), HB);
+    const uint32_t p0 = qb - boff;  // position of byte 0 (may be below the tile start)
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-      const uint32_t p = base + i;
-      if (p >= lim) break;
-      if (i < 15 && p + 1 < lim && h[i] == h[i + 1]) continue;
-      atomicMax(&tbl[h[i]], p);
+      const bool in = p0 + i >= t.start && p0 + i < lim;
+      const bool next_in = i < 15 && p0 + i + 1 >= t.start && p0 + i + 1 < lim;
+      if (in && !(next_in && h[i] == h[i + 1])) atomicMax(&tbl[h[i]], p0 + i);
     }
   }
   __syncthreads();
