@@ -26,11 +26,11 @@ constexpr const char* kGeometrySource = "orot_b200.tune on NVIDIA B200, 148 SMs,
 constexpr GeometryRow kGeometry[] = {
     {0ull, 4096, 8192, {1, 1, 1}},
     {1ull << 20, 4096, 8192, {2, 2, 2}},
-    {4ull << 20, 8192, 8192, {8, 8, 1}},
-    {16ull << 20, 16384, 32768, {4, 4, 2}},
-    {64ull << 20, 32768, 32768, {8, 8, 4}},
-    {256ull << 20, 32768, 65536, {16, 16, 16}},
-    {1ull << 30, 65536, 65536, {32, 32, 16}},
+    {4ull << 20, 4096, 8192, {8, 8, 1}},
+    {16ull << 20, 16384, 16384, {4, 4, 4}},
+    {64ull << 20, 16384, 16384, {16, 8, 4}},
+    {256ull << 20, 32768, 32768, {16, 16, 16}},
+    {1ull << 30, 32768, 65536, {32, 32, 16}},
     {4ull << 30, 65536, 65536, {32, 32, 16}},
 };
 
