@@ -800,7 +800,7 @@ def main():
             raise SystemExit("end-to-end sizes differ from the device-resident pass")
         e2e = {"value": world * total / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": total,
                "d2h_bytes_per_step": int(comp) + 16 * (len(sizes) + 1), "ms_per_step": dt * 1e3,
-               "api": "deflate_gpu_compress_pipelined (pinned host buffers, 512 MiB groups, 4 passes in flight)"}
+               "api": "deflate_gpu_compress_pipelined (pinned host buffers, 256 MiB groups, 6 passes in flight)"}
         if world == 1:
             # the same call from pageable (not pinned) input and output memory
             pin = np.empty(total, np.uint8)

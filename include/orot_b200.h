@@ -189,7 +189,7 @@ size_t deflate_gpu_packed_bound(const size_t* in_sizes, size_t count, deflate_fo
 
 /* Pipelined host-to-host batch (no counterpart in the reference): as
  * deflate_gpu_compress_packed, but the buffers are split into groups of about
- * group_bytes (0 = 512 MiB) and `lanes` passes (0 = 4) are kept in flight, so
+ * group_bytes (0 = 256 MiB) and `lanes` passes (0 = 6) are kept in flight, so
  * the copies of one group overlap the kernels of another.  Group g's outputs
  * start at the sum of the packed bounds of groups before it; out_offsets[i]
  * are absolute, out_offsets[count] is the end of the last output.  Returns

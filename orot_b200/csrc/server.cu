@@ -427,13 +427,15 @@ size_t deflate_gpu_compress_pipelined(const void* in_concat, const size_t* in_si
   const int dev = current_device();
   if (dev < 0) return 0;
   std::vector<Lane*>& pool = pools[dev];
-  const int nl = lanes > 0 ? std::min(lanes, 8) : 4;
+  const int nl = lanes > 0 ? std::min(lanes, 8) : 6;
   while (int(pool.size()) < nl) {
     Lane* L = new (std::nothrow) Lane();
     if (!L || !L->eng.ok) { delete L; set_error("lane set-up failed"); return 0; }
     pool.push_back(L);
   }
-  if (!group_bytes) group_bytes = size_t(512) << 20;
+  // defaults measured on B200 over PCIe 5 (10,000 buffers, 5.13 GB): 256 MiB
+  // groups with 6 lanes keep both copy directions busier than 512 MiB with 4
+  if (!group_bytes) group_bytes = size_t(256) << 20;
   // groups: contiguous buffer ranges
   std::vector<size_t> gfirst, gcount;
   std::vector<uint64_t> gsrc, gdst, gcap;
