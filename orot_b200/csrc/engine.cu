@@ -177,7 +177,9 @@ Engine::~Engine() {
 // pass at once; large tiles carry fewer head tables (4 B per entry: 16 KB
 // at 12 hash bits, 64 KB at 14) and fix up fewer boundaries.
 const GeometryRow& Engine::geometry(uint64_t total_bytes) const {
-  const uint64_t scaled = total_bytes / uint64_t(std::max(sms, 1)) * 148u;
+  // scaled to a 148-SM device (multiplied first: a pass of exactly a class
+  // boundary belongs to that class)
+  const uint64_t scaled = total_bytes * 148u / uint64_t(std::max(sms, 1));
   size_t k = 0;
   for (size_t i = 0; i < sizeof(kGeometry) / sizeof(kGeometry[0]); ++i)
     if (scaled >= kGeometry[i].min_bytes) k = i;
