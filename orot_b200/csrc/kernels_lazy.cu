@@ -423,15 +423,16 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
 
     // -- links of the new positions [lstart, nreg): the previous position
     // with the same 15-bit hash.  (1) All warps, 32-position chunks: the
-    // nearest earlier lane with the same hash is the link inside the chunk,
-    // and the first and last lane of every hash are marked.  (2) Warp 0,
-    // chunk after chunk: first lanes link to the table's position, last
-    // lanes replace it.  Only step (2) is sequential, and it does one table
-    // read and one table write per distinct hash.
+    // nearest earlier lane with the same hash is the link inside the chunk;
+    // the first lane of every hash is marked and, until step (2), holds in
+    // its link the offset to the hash's last lane in the chunk.  (2) Warp 0,
+    // chunk after chunk: each first lane reads the table's position (its
+    // link) and writes its hash's last position in the chunk.  Only step (2)
+    // is sequential: one table read and write per distinct hash, by one lane,
+    // and one warp barrier per chunk (the next chunk's reads come after).
     {
       const uint32_t nch = (nreg - lstart + 31) / 32;
       uint32_t* fbits = F;  // F is free until the searches
-      uint32_t* lbits = F + nch;
       const uint32_t lt = (1u << lane) - 1;
       for (uint32_t c = wid; c < nch; c += blockDim.x >> 5) {
         const uint32_t x = lstart + c * 32 + lane;
@@ -439,35 +440,36 @@ __global__ void __launch_bounds__(1024, 1) k_lz(Work wk, const uint32_t* __restr
         const uint32_t h = valid ? hash15(sd.load4(x)) : 0x10000u + lane;  // invalid lanes match nobody
         const uint32_t peers = __match_any_sync(kAll, h);
         const uint32_t before = peers & lt;
-        if (x < nreg) link[x] = before ? uint16_t(__clz(before) - (31 - lane)) : uint16_t(0);
-        const uint32_t first = __ballot_sync(kAll, valid && !before);
-        const uint32_t last = __ballot_sync(kAll, valid && !(peers & ~lt & ~(1u << lane)));
-        if (lane == 0) {
-          fbits[c] = first;
-          lbits[c] = last;
-        }
+        const bool is_first = valid && !before;
+        if (x < nreg)
+          link[x] = before ? uint16_t(__clz(before) - (31 - lane))
+                           : is_first ? uint16_t((31 - __clz(peers)) - lane) : uint16_t(0);
+        const uint32_t first = __ballot_sync(kAll, is_first);
+        if (lane == 0) fbits[c] = first;
       }
       __syncthreads();
       if (wid == 0) {
-        // eight chunks per round: their marks and hashes are loaded first,
-        // then the table reads and writes go in chunk order without waiting
-        // for each other's results
+        // eight chunks per round: their marks, hashes and last positions are
+        // loaded first, then the table reads and writes go in chunk order
+        // without waiting for each other's results
         constexpr uint32_t U = 8;
         for (uint32_t c0 = 0; c0 < nch; c0 += U) {
-          uint32_t fb[U], lb[U], h[U], p[U];
+          uint32_t fb[U], h[U], p[U], lastp[U];
+#pragma unroll
+          for (uint32_t u = 0; u < U; ++u) fb[u] = c0 + u < nch ? (fbits[c0 + u] >> lane) & 1u : 0u;
 #pragma unroll
           for (uint32_t u = 0; u < U; ++u) {
-            fb[u] = c0 + u < nch ? (fbits[c0 + u] >> lane) & 1u : 0u;
-            lb[u] = c0 + u < nch ? (lbits[c0 + u] >> lane) & 1u : 0u;
+            const uint32_t x = lstart + (c0 + u) * 32 + lane;
+            h[u] = fb[u] ? hash15(sd.load4(x)) : 0u;
+            lastp[u] = fb[u] ? x + link[x] : 0u;
           }
 #pragma unroll
-          for (uint32_t u = 0; u < U; ++u)
-            h[u] = (fb[u] | lb[u]) ? hash15(sd.load4(lstart + (c0 + u) * 32 + lane)) : 0u;
-#pragma unroll
           for (uint32_t u = 0; u < U; ++u) {
-            p[u] = fb[u] ? uint32_t(tbl[h[u]]) : 0xFFFFu;
-            __syncwarp();
-            if (lb[u]) tbl[h[u]] = uint16_t(lstart + (c0 + u) * 32 + lane);
+            p[u] = 0xFFFFu;
+            if (fb[u]) {
+              p[u] = tbl[h[u]];
+              tbl[h[u]] = uint16_t(lastp[u]);
+            }
             __syncwarp();
           }
 #pragma unroll
