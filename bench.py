@@ -466,7 +466,7 @@ def measure_serving(deflate, buf, total, count, rate, cap_count, seed=0):
 # input byte, for the issue-rate roofline (4 warp instructions per SM cycle).
 # The "parse" phase is k_cand_parse, the candidate pass and the parse in one
 # kernel (the "candidates" phase is empty then).
-WARP_INST_PER_BYTE = {"candidates": 3.65, "parse": 12.07, "lazy_match": 79.3}
+WARP_INST_PER_BYTE = {"candidates": 3.65, "parse": 12.07, "lazy_match": 77.4}
 PHASE_KERNEL = {"candidates": "k_cand", "parse": "k_cand_parse",  "lazy_match": "k_lz", "lazy_encode": "k_enc", "lazy_huffman": "k_huff",
                 "hash_carry": "k_lastocc + k_carry_scan", "fixup": "k_fix1 + k_fix2", "join": "k_join",
                 "checksum": "k_ck_block + k_ck_fold", "plan": "k_plan + k_zero"}
