@@ -289,6 +289,12 @@ const char* orot_b200_last_error(void);
  * the hand-set rules it starts from (no counterpart in the reference). */
 const char* orot_b200_geometry_source(void);
 
+/* Tile bytes the planner uses at levels 1-3 (hash_bits 12: level 1; 14:
+ * levels 2-3) for a pass of `pass_bytes` input bytes on a device of `sms`
+ * SMs, from the compiled geometry table (no counterpart in the reference;
+ * needs no GPU).  OROT_B200_TILE, when set, overrides it in a pass. */
+uint32_t orot_b200_geometry_tile(uint64_t pass_bytes, int sms, int hash_bits);
+
 #ifdef __cplusplus
 }
 #endif

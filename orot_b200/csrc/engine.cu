@@ -176,15 +176,18 @@ Engine::~Engine() {
 // with proportionally less input.  Small tiles let more warps walk a small
 // pass at once; large tiles carry fewer head tables (4 B per entry: 16 KB
 // at 12 hash bits, 64 KB at 14) and fix up fewer boundaries.
-const GeometryRow& Engine::geometry(uint64_t total_bytes) const {
-  // scaled to a 148-SM device (multiplied first: a pass of exactly a class
-  // boundary belongs to that class)
+// The table row of a pass of `total_bytes` on a device of `sms` SMs: sizes
+// are scaled to a 148-SM device (multiplied first, so that a pass of exactly
+// a class boundary belongs to that class).
+static const GeometryRow& geometry_row(uint64_t total_bytes, int sms) {
   const uint64_t scaled = total_bytes * 148u / uint64_t(std::max(sms, 1));
   size_t k = 0;
   for (size_t i = 0; i < sizeof(kGeometry) / sizeof(kGeometry[0]); ++i)
     if (scaled >= kGeometry[i].min_bytes) k = i;
   return kGeometry[k];
 }
+
+const GeometryRow& Engine::geometry(uint64_t total_bytes) const { return geometry_row(total_bytes, sms); }
 
 uint32_t Engine::pick_tile(uint64_t total_bytes, int hash_bits) const {
   if (tile_override) return tile_override;
@@ -754,5 +757,10 @@ uint32_t deflate_adler32(uint32_t init, const void* data, size_t len) {
 
 const char* orot_b200_last_error(void) { return g_err.c_str(); }
 const char* orot_b200_geometry_source(void) { return kGeometrySource; }
+
+uint32_t orot_b200_geometry_tile(uint64_t pass_bytes, int sms, int hash_bits) {
+  const GeometryRow& g = geometry_row(pass_bytes, sms);
+  return hash_bits <= 12 ? g.tile12 : g.tile14;
+}
 
 }  // extern "C"

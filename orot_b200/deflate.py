@@ -68,6 +68,8 @@ def lib() -> ctypes.CDLL:
     L.deflate_adler32.argtypes = [c.c_uint32, c.c_void_p, c.c_size_t]
     L.orot_b200_last_error.restype = c.c_char_p
     L.orot_b200_geometry_source.restype = c.c_char_p
+    L.orot_b200_geometry_tile.restype = c.c_uint32
+    L.orot_b200_geometry_tile.argtypes = [c.c_uint64, c.c_int, c.c_int]
     L.deflate_gpu_batch_new.restype = c.c_void_p
     L.deflate_gpu_batch_free.argtypes = [c.c_void_p]
     L.deflate_gpu_batch_load.restype = c.c_int
@@ -143,6 +145,12 @@ def last_error() -> str:
 def geometry_source() -> str:
     """Where the library's pass geometry table came from (the autotuner's run)."""
     return lib().orot_b200_geometry_source().decode()
+
+
+def geometry_tile(pass_bytes: int, sms: int = 148, hash_bits: int = 12) -> int:
+    """Tile bytes the planner uses at levels 1-3 for a pass of `pass_bytes`
+    on a device of `sms` SMs (hash_bits 12: level 1, 14: levels 2-3)."""
+    return int(lib().orot_b200_geometry_tile(int(pass_bytes), int(sms), int(hash_bits)))
 
 
 def _ptr(buf) -> tuple[int, int, object]:
