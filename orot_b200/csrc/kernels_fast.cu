@@ -24,10 +24,16 @@
 //                 The parse starts at the tile's first byte (speculation) and
 //                 one record per 32 positions remembers where it entered that
 //                 window; windows a match covers cost only that record.
-//   k_fixup       one warp per multi-tile segment, tiles in order: re-walks a
-//                 tile from the true entry (where the previous tile's parse
-//                 ended) until it meets the speculative parse at a window
-//                 boundary; from there the speculative bits are exact.
+//   k_cand_parse  (the default) both passes in one persistent kernel: 16
+//                 walkers (4 at 14 hash bits) and the rest of 32 warps as
+//                 parsers per SM; a parser takes a tile once a walker has
+//                 published its candidates.
+//   k_fix1/k_fix2 re-walk a tile from the true entry (where the previous
+//                 tile's parse ended; k_fix1 all tiles at once assuming the
+//                 previous speculation held, k_fix2 one warp per multi-tile
+//                 segment, tiles in order, where it did not) until it
+//                 meets the speculative parse at a window boundary; from
+//                 there the speculative bits are exact.
 //
 // The output is therefore token-for-token the reference's.
 #include <cuda_runtime.h>
